@@ -1,0 +1,385 @@
+"""Benchmark of the heatbath + Wilson-flow hot path on the 32^4 precision workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step"): a 32^4 lattice, Haar hot start from seed 7, 500 checkerboard
+Cabibbo-Marinari heatbath sweeps at beta = 6.0 (N_hits = 1), then Wilson flow to t = 4
+(200 RK3 steps of eps = 0.02) with clover Q/E recorded every 10 steps; links stored as FP32
+12-real, reductions in FP64.  The 32^4 FP32 field is 201 MB, larger than the 126 MB L2, so
+no L2 flush is needed between timed iterations.
+
+`value` is heatbath link-updates/s over the timed steps (CUDA events on the library's
+stream, max over ranks); the flow rate, the FP64 path, the FP32-vs-FP64 errors and the
+roofline of the dominant kernel are reported beside it.  `e2e` repeats the step through
+the C ABI from a pinned host buffer of FP64 links (set_links) with results read back.
+
+--impl reference times the reference algorithm on the host cores: the oracle's CPU
+restatement (the reference itself cannot be built: no MPI, Eigen or c-lime) with the
+reference schedule (frozen links, random shifts, lexicographic sweeps), one process per
+core on 16^4 blocks as the reference's 2^4-rank decomposition of 32^4 would run.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "ecmc-qncb_b200"))
+
+L = 32
+BETA = 6.0
+SEED = 7
+SWEEPS = 500
+FLOW_EPS = 0.02
+FLOW_RECORDS, FLOW_RK = 20, 10          # 200 RK3 steps, Q/E every 10
+METRIC = "HB link-updates/s; flow site-steps/s; FP32 vs FP64 @|ΔQ|<1e-4; p99 latency"
+
+# Algorithmic bytes (compulsory HBM traffic) per unit, by storage (bytes per link b):
+# heatbath pass: read all 4V links once + write the V/2 updated ones = 9 b per link-update;
+# flow: 24 link records + 16 su(3) records (8 reals) per site-step.
+HB_BYTES = {("fp32", 12): 9 * 48, ("fp32", 18): 9 * 72, ("fp64", 18): 9 * 144}
+FLOW_BYTES = {("fp32", 12): 24 * 48 + 16 * 32, ("fp64", 18): 24 * 144 + 16 * 64}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the dominant kernels from the committed ncu summaries."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return {}
+    return {}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"qcb_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not self.path.exists():
+            return None
+        rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.count(",") >= 8]
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------------------
+def run_ours(args, rank: int, world: int, local_rank: int, dist):
+    import numpy as np
+    import torch
+
+    import qcb
+    from qcb import _lib
+
+    torch.cuda.set_device(local_rank)
+    ctx = qcb.Context(local_rank)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local_rank))
+    lib = _lib.lib()
+    dims = (L, L, L, L)
+    V = L ** 4
+    seed = SEED + 1000 * rank  # independent replicas per rank
+
+    f32 = qcb.GaugeField(ctx, dims, "fp32", 12)
+    gf = qcb.GradientFlow(FLOW_EPS)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def step(field, hb_ev=None):
+        field.hot_start(seed)
+        if hb_ev:
+            hb_ev[0].record(stream)
+        _lib.check(lib.qcb_heatbath(field.h, BETA, SWEEPS, 1, seed, 0))
+        if hb_ev:
+            hb_ev[1].record(stream)
+        return qcb.observables.topo_charge_flowed(field, gf, FLOW_RECORDS, FLOW_RK)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step(f32)
+    ctx.sync()
+
+    # ---- timed region: K steps -------------------------------------------------------
+    hb_events = [(ev(), ev()) for _ in range(args.steps)]
+    t0, t1 = ev(), ev()
+    launches0 = ctx.launches()
+    barrier()
+    with Clocks(local_rank) as clk:
+        t0.record(stream)
+        for k in range(args.steps):
+            step(f32, hb_events[k])
+        t1.record(stream)
+        barrier()
+    ctx.sync()
+    launches = ctx.launches() - launches0
+    total_ms = t0.elapsed_time(t1)
+    hb_ms = sum(a.elapsed_time(b) for a, b in hb_events)
+    flow_ms = total_ms - hb_ms  # hot start + flow + measurements
+    total_ms = max_over_ranks(total_ms)
+    hb_ms = max_over_ranks(hb_ms)
+    flow_ms = max_over_ranks(flow_ms)
+    updates = world * args.steps * SWEEPS * 4 * V
+    site_steps = world * args.steps * FLOW_RECORDS * FLOW_RK * V
+    hb_rate = updates / (hb_ms / 1e3)
+    flow_rate = site_steps / (flow_ms / 1e3)
+
+    # ---- per-launch durations of the dominant kernels (roofline) --------------------------
+    def per_launch(fn, n):
+        evs = [(ev(), ev()) for _ in range(n)]
+        for a, b in evs:
+            a.record(stream)
+            fn()
+            b.record(stream)
+        torch.cuda.synchronize()
+        return statistics.mean(a.elapsed_time(b) for a, b in evs)
+
+    f32.hot_start(seed)
+    # one heatbath sweep = 8 pass launches
+    hb_sweep_ms = per_launch(lambda: _lib.check(lib.qcb_heatbath(f32.h, BETA, 1, 1, seed, 0)), 20)
+    hb_pass_ms = hb_sweep_ms / 8
+    rk3_ms = per_launch(lambda: _lib.check(lib.qcb_flow_steps(f32.h, FLOW_EPS, 1)), 10)
+    peak, peak_kind = peaks()
+    hb_bytes_launch = HB_BYTES[("fp32", 12)] * V / 2
+    hb_achieved = hb_bytes_launch / (hb_pass_ms / 1e3) / 1e9
+    flow_achieved = FLOW_BYTES[("fp32", 12)] * V / (rk3_ms / 1e3) / 1e9
+    traffic = ncu_traffic()
+
+    # ---- FP64 path (same workload, one untimed-for-value step) ---------------------------
+    f64 = qcb.GaugeField(ctx, dims, "fp64", 18)
+    e64 = (ev(), ev())
+    a64, b64 = ev(), ev()
+    a64.record(stream)
+    step(f64, e64)
+    b64.record(stream)
+    ctx.sync()
+    hb64_ms = e64[0].elapsed_time(e64[1])
+    flow64_ms = a64.elapsed_time(b64) - hb64_ms
+    hb64_rate = SWEEPS * 4 * V / (hb64_ms / 1e3)
+    flow64_rate = FLOW_RECORDS * FLOW_RK * V / (flow64_ms / 1e3)
+
+    # ---- precision: FP32-12 flow vs FP64-18 flow of the same FP64 heatbath output ----------
+    f64.hot_start(seed)
+    _lib.check(lib.qcb_heatbath(f64.h, BETA, SWEEPS, 1, seed, 0))
+    f32.copy_from(f64)
+    p64 = qcb.observables.mean_plaquette_global(f64)
+    p32 = qcb.observables.mean_plaquette_global(f32)
+    r64 = qcb.observables.topo_charge_flowed(f64, gf, 21, 10).reshape(-1, 3)
+    r32 = qcb.observables.topo_charge_flowed(f32, gf, 21, 10).reshape(-1, 3)
+    precision = {"dP": abs(p32 - p64), "dQ_max": float(np.abs(r32[:, 1] - r64[:, 1]).max()),
+                 "dE_rel_max": float((np.abs(r32[:, 2] - r64[:, 2]) / np.abs(r64[:, 2])).max()),
+                 "Q_t4_fp64": float(r64[-1, 1]), "E_t4_fp64": float(r64[-1, 2]), "plaquette_fp64": p64,
+                 "same_input": "FP64 heatbath output, flowed in FP32-12 and in FP64-18"}
+
+    # ---- e2e through the C ABI with host buffers ------------------------------------------
+    host = torch.empty(V * 72, dtype=torch.float64).pin_memory()
+    host.copy_(torch.from_numpy(f64.get_links().view(np.float64).reshape(-1)))
+    tqe_host = np.zeros(3 * FLOW_RECORDS)
+    e2e_ms = []
+    for k in range(args.warmup + args.steps):
+        barrier()
+        a, b = ev(), ev()
+        a.record(stream)
+        f32.set_links_ptr(host.data_ptr())
+        _lib.check(lib.qcb_heatbath(f32.h, BETA, SWEEPS, 1, seed, 0))
+        tqe_host[:] = qcb.observables.topo_charge_flowed(f32, gf, FLOW_RECORDS, FLOW_RK)
+        plaq = qcb.observables.mean_plaquette_global(f32)
+        b.record(stream)
+        b.synchronize()
+        if k >= args.warmup:
+            e2e_ms.append(a.elapsed_time(b))
+    e2e_step_ms = max_over_ranks(statistics.mean(e2e_ms))
+    e2e_rate = world * SWEEPS * 4 * V / (e2e_step_ms / 1e3)
+    assert np.isfinite(plaq)
+
+    result = {
+        "metric": METRIC, "value": hb_rate, "unit": "link-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 links, f64 reductions", "data": "synthetic",
+        "config": {"workload": "precision 32^4: Haar hot start seed 7, 500 CM heatbath sweeps beta=6.0, "
+                               "flow to t=4 (200 RK3 eps=0.02, Q/E every 10)",
+                   "lattice": [L, L, L, L], "storage": "fp32-12", "sweeps": SWEEPS, "n_hits": 1,
+                   "flow_steps": FLOW_RECORDS * FLOW_RK, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (201 MB field vs 126 MB L2); no flush"},
+        "flow": {"value": flow_rate, "unit": "site-steps/s", "ms_per_rk3": rk3_ms,
+                 "roofline": {"bound": "hbm", "achieved": flow_achieved, "peak": peak, "unit": "GB/s",
+                              "frac": flow_achieved / peak, "peak_kind": peak_kind,
+                              "traffic": traffic.get("flow_stage_fp32r12_per_rk3")}},
+        "fp64": {"hb_value": hb64_rate, "flow_value": flow64_rate, "storage": "fp64-18",
+                 "hb_speedup_fp32": hb_rate / world / hb64_rate, "flow_speedup_fp32": flow_rate / world / flow64_rate},
+        "precision": precision,
+        "roofline": {"bound": "hbm", "kernel": "k_hb_pass<float,12>", "achieved": hb_achieved, "peak": peak,
+                     "unit": "GB/s", "frac": hb_achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic.get("hb_pass_fp32r12_per_launch"),
+                     "algorithmic_bytes_per_launch": hb_bytes_launch, "launch_ms": hb_pass_ms},
+        "e2e": {"value": e2e_rate, "unit": "link-updates/s", "ms_per_step": e2e_step_ms,
+                "h2d_bytes_per_step": V * 72 * 8, "d2h_bytes_per_step": (3 * FLOW_RECORDS + 1) * 8},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    return result
+
+
+# ---------------------------------------------------------------------------------------
+def _ref_worker(args):
+    """One 'rank' of the reference schedule on a block of edge lb: sweeps then flow."""
+    lb, sweeps, rk3, seed = args
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    chain = oracle.RefChain(lb, seed, False)
+    t = time.perf_counter()
+    chain.run(BETA, sweeps, 1, 1)  # shift + sweep + plaquette per shift
+    t_hb = time.perf_counter() - t
+    dims = (lb,) * 4
+    u = chain.links()
+    t = time.perf_counter()
+    oracle.flow_steps(u, dims, FLOW_EPS, rk3)
+    t_flow = time.perf_counter() - t
+    return t_hb, chain.updates_per_sweep() * sweeps, t_flow, lb ** 4 * rk3
+
+
+def cpu_baseline(sweeps: int = 1, rk3: int = 1, block: int = 16):
+    """Reference algorithm on the host cores: one process per core (the reference runs
+    one MPI rank per core), each on a 16^4 block of the 32^4 lattice."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    oracle.build()
+    cores = min(16, os.cpu_count() or 1)
+    with mp.get_context("spawn").Pool(cores) as pool:
+        t = time.perf_counter()
+        res = pool.map(_ref_worker, [(block, sweeps, rk3, 100 + r) for r in range(cores)])
+        wall = time.perf_counter() - t
+    hb_rate = sum(r[1] for r in res) / max(r[0] for r in res)
+    flow_rate = sum(r[3] for r in res) / max(r[2] for r in res)
+    return {"value": hb_rate, "unit": "link-updates/s", "cores": cores, "kind": "port",
+            "flow_value": flow_rate, "flow_unit": "site-steps/s", "wall_s": wall,
+            "sample": f"{cores} processes x ({sweeps} reference shift+sweep on a {block}^4 block with frozen "
+                      f"links, then {rk3} RK3 flow step); link-updates counted as 4L(L-1)^3 per sweep"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        runs = []
+        for _ in range(args.warmup + args.steps):
+            runs.append(cpu_baseline())
+        timed = runs[args.warmup:]
+        v = statistics.mean(r["value"] for r in timed)
+        cb = dict(timed[0])
+        cb["value"] = v
+        out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "link-updates/s", "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": "precision 32^4 (reference schedule, 16^4 blocks per core), beta=6.0, "
+                                      "hot start; sweep and RK3 flow rates", "lattice": [L, L, L, L]},
+               "flow": {"value": statistics.mean(r["flow_value"] for r in timed), "unit": "site-steps/s"},
+               "cpu_baseline": cb,
+               "e2e": {"value": v, "unit": "link-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(out))
+        return 0
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                 device_id=torch.device("cuda", local_rank))
+        dist = tdist
+    try:
+        res = run_ours(args, rank, world, local_rank, dist)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            res["cpu_baseline"] = cpu_baseline()
+        if rank == 0:
+            print(json.dumps(res))
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

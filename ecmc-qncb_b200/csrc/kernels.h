@@ -1,0 +1,59 @@
+// kernels.h — host-side launchers of the sm_100a kernels (one .cu file per family).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "layout.cuh"
+
+namespace qcb {
+
+// Device description of one lattice's link storage.
+struct LatDev {
+  Geom g;
+  int prec;   // QCB_FP64 / QCB_FP32
+  int nr;     // 18 / 12
+  void* links;
+};
+
+// Device description of one su(3) algebra field (flow accumulator), same precision.
+struct AlgDev {
+  void* p;
+};
+
+size_t link_bytes(const Geom& g, int prec, int nr);
+size_t alg_bytes(const Geom& g, int prec);
+Geom make_geom(const int dims[4]);
+
+// ---- util (k_util.cu) --------------------------------------------------------------
+cudaError_t launch_cold(const LatDev& L, cudaStream_t s, int block);
+cudaError_t launch_hot(const LatDev& L, uint64_t seed, cudaStream_t s, int block);
+cudaError_t launch_gauge_transform(const LatDev& L, uint64_t seed, cudaStream_t s, int block);
+cudaError_t launch_reunitarize(const LatDev& L, cudaStream_t s, int block);
+// AoS FP64 (72 doubles per site, ILDG order) for the t-slab [t0, t0+nt) <-> lattice.
+cudaError_t launch_aos_to_soa(const LatDev& L, const double* aos, int t0, int nt, int bswap, cudaStream_t s,
+                              int block);
+cudaError_t launch_soa_to_aos(const LatDev& L, double* aos, int t0, int nt, int bswap, cudaStream_t s,
+                              int block);
+cudaError_t launch_convert(const LatDev& dst, const LatDev& src, cudaStream_t s, int block);
+
+// ---- heatbath (k_hb.cu) ------------------------------------------------------------
+// One checkerboard pass: every link (mu, parity) gets n_hits Cabibbo-Marinari hits.
+// status[0] counts KP draws that hit the attempt cap.
+cudaError_t launch_hb_pass(const LatDev& L, int mu, int parity, double beta, uint64_t seed, uint32_t sweep,
+                           int n_hits, uint32_t* status, cudaStream_t s, int block);
+
+// ---- observables (k_obs.cu) --------------------------------------------------------
+// Reductions write per-block partial sums into scratch (nparts doubles per quantity,
+// nparts = reduce_blocks()) and a final single-block kernel writes the FP64 total(s)
+// into out (device).
+int reduce_blocks();
+cudaError_t launch_plaquette(const LatDev& L, double* scratch, double* out, cudaStream_t s, int block);
+cudaError_t launch_clover_qe(const LatDev& L, double* scratch, double* out2, cudaStream_t s, int block);
+
+// ---- flow (k_flow.cu) --------------------------------------------------------------
+// RK3 stage k (1, 2, 3) of Luescher's integrator: reads links from src, the force
+// accumulator z, writes links to dst.
+cudaError_t launch_flow_stage(int stage, const LatDev& src, const LatDev& dst, const AlgDev& z, double eps,
+                              cudaStream_t s, int block);
+
+}  // namespace qcb

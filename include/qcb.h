@@ -1,0 +1,165 @@
+/*
+ * qcb.h — C ABI of the B200 (sm_100a) implementation of the ECMC-QNCB heatbath /
+ * plaquette / Wilson-flow hot path.
+ *
+ * Conventions
+ *   - Every function returns int: QCB_OK (0) or an error code; qcb_last_error()
+ *     returns the message of the last failure on the calling thread.
+ *   - No C++ exception crosses this boundary.
+ *   - An opaque qcb_ctx binds one CUDA device and one stream; a qcb_lattice owns its
+ *     device memory.  Calls on one context are serialised in stream order; different
+ *     contexts may be driven from different threads.
+ *   - Host buffers are owned by the caller and only borrowed for the duration of a call.
+ *   - Host link buffers ("AoS") use the ILDG site order of the reference
+ *     (src/io/ildg.cpp:87-106): t slowest, then z, y, x; per site mu = 0..3; per link a
+ *     row-major 3x3 of (re, im) doubles, i.e. 72 doubles per site, native endian.
+ *
+ * The reference exposes no FFI; each entry point names the reference function whose
+ * role it takes over (file:line within the reference project).
+ */
+#ifndef QCB_H
+#define QCB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QCB_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------------------- */
+enum {
+  QCB_OK = 0,
+  QCB_ERR_INVALID = 1,   /* bad argument (null pointer, odd extent, bad enum, ...)      */
+  QCB_ERR_CUDA = 2,      /* a CUDA runtime call failed (no device, launch error, ...)   */
+  QCB_ERR_IO = 3,        /* file could not be opened / read / written                   */
+  QCB_ERR_FORMAT = 4,    /* malformed LIME/ILDG file or input file value                */
+  QCB_ERR_NOMEM = 5,     /* device or host allocation failed / admission refused        */
+  QCB_ERR_KP_CAP = 6,    /* Kennedy-Pendleton rejection loop hit its attempt cap        */
+  QCB_ERR_STATE = 7,     /* call not valid in the current object state                  */
+  QCB_ERR_CANCELLED = 8  /* serving job cancelled before completion                     */
+};
+
+/* ---- enums ------------------------------------------------------------------------ */
+enum { QCB_FP64 = 0, QCB_FP32 = 1 };           /* arithmetic / storage precision        */
+enum { QCB_R18 = 18, QCB_R12 = 12 };           /* reals stored per link                 */
+
+typedef struct qcb_ctx qcb_ctx;
+typedef struct qcb_lattice qcb_lattice;
+
+/* ---- library ---------------------------------------------------------------------- */
+int qcb_abi_version(void);
+const char* qcb_last_error(void);
+/* Number of CUDA devices visible (0 on a host without GPU; never fails). */
+int qcb_device_count(int* count);
+
+/* ---- context ------------------------------------------------------------------------
+ * Replaces the per-rank process state of the reference driver
+ * (src/bin/gauge_hb_ncb.cpp:18-28: MpiTopology + GeometryCB + RNG). */
+int qcb_ctx_create(int device, unsigned flags, qcb_ctx** out);
+int qcb_ctx_destroy(qcb_ctx* ctx);
+/* Waits for all work queued on the context's stream, then reports device-side
+ * status words (KP cap hits) accumulated since the last call. */
+int qcb_ctx_sync(qcb_ctx* ctx);
+/* Number of kernels this context launched so far (all kinds). */
+int qcb_ctx_launch_count(qcb_ctx* ctx, uint64_t* count);
+/* Thread-block size used by subsequent launches of the per-link/per-site kernels
+ * (0 = built-in default).  Results do not depend on it. */
+int qcb_ctx_set_block(qcb_ctx* ctx, int threads);
+/* The cudaStream_t the context launches on (as void*). */
+int qcb_ctx_stream(qcb_ctx* ctx, void** stream);
+
+/* ---- lattice ------------------------------------------------------------------------
+ * Replaces GaugeField + GeometryCB (src/gauge/GaugeField.h:18-62,
+ * src/geometry/GeometryCB.h:8-58): periodic lattice of extents dims = {Lx,Ly,Lz,Lt}
+ * (all even, >= 2), stored on the device in a parity-split structure-of-arrays layout.
+ * A new lattice is cold (every link the identity, GaugeField.h:37-42). */
+int qcb_lattice_create(qcb_ctx* ctx, const int dims[4], int precision, int storage,
+                       qcb_lattice** out);
+int qcb_lattice_destroy(qcb_lattice* lat);
+int qcb_lattice_info(const qcb_lattice* lat, int dims[4], int* precision, int* storage,
+                     size_t* device_bytes);
+/* Device address of the link storage and its layout parameters (for zero-copy users):
+ * chunk c of link (mu, parity, i) sits at element ((mu*2+parity)*nchunk + c)*stride + i
+ * of an array of chunk-sized vectors (double2, float4 or float2). */
+int qcb_lattice_device_links(const qcb_lattice* lat, void** dev_ptr, size_t* stride,
+                             int* nchunk, int* chunk_bytes);
+
+/* GaugeField::cold_start (src/gauge/GaugeField.cpp:23-34). */
+int qcb_cold_start(qcb_lattice* lat);
+/* GaugeField::hot_start (src/gauge/GaugeField.cpp:10-20), redesigned: every link drawn
+ * Haar-uniformly in SU(3) from a Philox4x32-10 stream keyed by seed. */
+int qcb_hot_start(qcb_lattice* lat, uint64_t seed);
+/* Copy links from / to a host AoS FP64 buffer (72*V doubles, ILDG order, native endian);
+ * replaces the pack/unpack loops of src/io/ildg.cpp:87-106,212-232. */
+int qcb_set_links(qcb_lattice* lat, const double* aos);
+int qcb_get_links(qcb_lattice* lat, double* aos);
+/* Copy src into dst (same dims; precision/storage may differ: converts on the device). */
+int qcb_copy_links(qcb_lattice* dst, const qcb_lattice* src);
+/* Reunitarise every link (Gram-Schmidt on rows 0,1; row 2 = conj(row0 x row1)).
+ * Reference counterpart: GaugeField::project_field_su3 (GaugeField.cpp:36-58), which uses
+ * columns; both map a near-SU(3) matrix to SU(3). */
+int qcb_reunitarize(qcb_lattice* lat);
+/* Random gauge transformation U_mu(x) -> G(x) U_mu(x) G(x+mu)^dagger with Haar G from
+ * seed (GaugeField::gauge_transform, GaugeField.cpp:100-114). */
+int qcb_gauge_transform(qcb_lattice* lat, uint64_t seed);
+
+/* ---- ILDG / LIME -------------------------------------------------------------------
+ * save_ildg_clime / read_ildg_clime (src/io/ildg.cpp:34-136, 138-237): a LIME file with an
+ * "ildg-format" XML record and an "ildg-binary-data" record of big-endian FP64 links.
+ * The lattice must be hypercubic (the reference's XML carries one extent). */
+int qcb_save_ildg(qcb_lattice* lat, const char* path);
+int qcb_load_ildg(qcb_lattice* lat, const char* path);
+/* Host-only: locate the binary record; returns its byte offset and length. */
+int qcb_ildg_probe(const char* path, uint64_t* data_offset, uint64_t* data_bytes);
+
+/* ---- heatbath ----------------------------------------------------------------------
+ * mpi::heatbathcb::samples / sweep / hit (src/heatbath/heatbath_mpi.cpp:11-69) with
+ * heatbath::su2_step / generate_su2_kp (src/heatbath/heatbath.cpp:8-44): n_sweeps sweeps of
+ * Cabibbo-Marinari updates over subgroups (0,1),(1,2),(0,2), n_hits hits per link, each
+ * sweep = 8 checkerboard passes (mu = 0..3, parity 0 then 1).  Random numbers come from
+ * Philox4x32-10 keyed by seed with counters (link, sweep_offset + s, hit/subgroup, draw),
+ * so the result does not depend on the launch shape.  Asynchronous: the KP status is
+ * reported by the next qcb_ctx_sync / result-returning call. */
+int qcb_heatbath(qcb_lattice* lat, double beta, int n_sweeps, int n_hits, uint64_t seed,
+                 uint64_t sweep_offset);
+
+/* ---- observables -------------------------------------------------------------------
+ * mpi::observables::mean_plaquette_global (src/observables/observables_mpi.cpp:8-43):
+ * sum_{x, mu<nu} Re tr P_{mu nu}(x) / 3, divided by 6V.  FP64 accumulation. */
+int qcb_plaquette(qcb_lattice* lat, double* out);
+/* topo_q_e_clover_global (observables_mpi.cpp:61-150): clover charge Q (total) and energy
+ * density E = (1/V) sum_x 1/2 sum_{mu<nu} |F_{mu nu}|^2 with F = (C - C^dagger)/8. */
+int qcb_topo_qe(qcb_lattice* lat, double* q, double* e);
+
+/* ---- Wilson flow -------------------------------------------------------------------
+ * mpi::observables::topo_charge_flowed (observables_mpi.cpp:153-178) with
+ * GradientFlow::rk3_step (src/flow/gradient_flow.cpp:15-128): on a copy of the links,
+ * for s < n_steps_gf: record (t, Q, E) into tQE[3s..3s+2], then n_rk_steps RK3 steps of
+ * size eps.  The lattice itself is left unchanged.  tQE holds 3*n_steps_gf doubles. */
+int qcb_flow_measure(qcb_lattice* lat, double eps, int n_steps_gf, int n_rk_steps,
+                     double* tQE);
+/* n RK3 steps of size eps applied to the lattice in place (no measurement). */
+int qcb_flow_steps(qcb_lattice* lat, double eps, int n);
+
+/* ---- input file ----------------------------------------------------------------------
+ * io::load_params(..., RunParamsHbCB&) (src/io/io.cpp:353-399) with the defaults of
+ * src/io/params.h:46-63.  Host-only.  Strings are NUL-terminated and truncated to fit. */
+typedef struct qcb_hb_params {
+  int L_core, n_core_dims, cold_start, N_switch_eo, N_shift, seed;
+  double beta;
+  int N_samples, N_hits, N_sweeps, N_therm;
+  int topo, N_shift_plaquette, N_shift_topo, N_steps_gf, N_rk_steps;
+  int save_each_shifts;
+  char run_name[256];
+  char run_dir[1024];
+} qcb_hb_params;
+int qcb_params_default(qcb_hb_params* p);
+int qcb_params_load(const char* path, qcb_hb_params* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QCB_H */

@@ -1,0 +1,320 @@
+"""ctypes loader for the FP64 CPU oracle (oracle/qcb_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline / reference arm, as the checker.  The product (libqcb and the qcb package) never
+imports it.  Parity unpinned: the reference itself cannot be built here (no MPI, Eigen or
+c-lime), so this restatement is checked against known answers, not reference outputs.
+
+Arrays use the ILDG site order of the reference: shape (Lt, Lz, Ly, Lx, 4, 3, 3) complex128,
+i.e. 72 doubles per site.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "liborc.so"
+
+_lib = None
+
+
+def build() -> Path:
+    """Compile liborc.so with the committed Makefile (g++, FP64, -O2)."""
+    subprocess.run(["make", "-s", "-f", str(HERE / "Makefile")], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+        u32p = C.POINTER(C.c_uint32)
+        L.orc_plaquette.argtypes = [dp, ip, dp]
+        L.orc_topo_qe.argtypes = [dp, ip, dp, dp]
+        L.orc_flow_measure.argtypes = [dp, ip, C.c_double, C.c_int, C.c_int, dp]
+        L.orc_flow_steps.argtypes = [dp, ip, C.c_double, C.c_int]
+        L.orc_staple.argtypes = [dp, ip, C.c_long, C.c_int, dp]
+        L.orc_exp_su3.argtypes = [dp, C.c_double, dp]
+        L.orc_proj_lie.argtypes = [dp, dp]
+        L.orc_philox.argtypes = [u32p, u32p, u32p]
+        L.orc_mt19937_64_nth.argtypes = [C.c_uint64, C.c_int]
+        L.orc_mt19937_64_nth.restype = C.c_uint64
+        L.orc_heatbath_cb.argtypes = [dp, ip, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_uint64]
+        L.orc_heatbath_cb.restype = C.c_uint64
+        L.orc_hot_start_philox.argtypes = [dp, ip, C.c_uint64]
+        L.orc_gauge_transform_philox.argtypes = [dp, ip, C.c_uint64]
+        L.orc_kp_samples.argtypes = [C.c_double, C.c_double, C.c_int, C.c_uint64, dp]
+        L.orc_ref_create.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.orc_ref_create.restype = C.c_void_p
+        L.orc_ref_destroy.argtypes = [C.c_void_p]
+        L.orc_ref_run.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int, dp]
+        L.orc_ref_sweeps.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int]
+        L.orc_ref_get_links.argtypes = [C.c_void_p, dp]
+        L.orc_ref_set_links.argtypes = [C.c_void_p, dp]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _dims(dims):
+    return (C.c_int * 4)(*dims)
+
+
+def shape(dims):
+    lx, ly, lz, lt = dims
+    return (lt, lz, ly, lx, 4, 3, 3)
+
+
+def cold(dims) -> np.ndarray:
+    u = np.zeros(shape(dims), np.complex128)
+    u[..., 0, 0] = u[..., 1, 1] = u[..., 2, 2] = 1.0
+    return u
+
+
+def hot_philox(dims, seed: int) -> np.ndarray:
+    u = np.zeros(shape(dims), np.complex128)
+    lib().orc_hot_start_philox(_dp(u), _dims(dims), C.c_uint64(seed))
+    return u
+
+
+def plaquette(u, dims) -> float:
+    u = np.ascontiguousarray(u, np.complex128)
+    out = C.c_double()
+    lib().orc_plaquette(_dp(u), _dims(dims), C.byref(out))
+    return out.value
+
+
+def topo_qe(u, dims):
+    u = np.ascontiguousarray(u, np.complex128)
+    q, e = C.c_double(), C.c_double()
+    lib().orc_topo_qe(_dp(u), _dims(dims), C.byref(q), C.byref(e))
+    return q.value, e.value
+
+
+def flow_measure(u, dims, eps, n_steps_gf, n_rk_steps) -> np.ndarray:
+    u = np.ascontiguousarray(u, np.complex128)
+    out = np.zeros(3 * n_steps_gf)
+    lib().orc_flow_measure(_dp(u), _dims(dims), eps, n_steps_gf, n_rk_steps, _dp(out))
+    return out
+
+
+def flow_steps(u, dims, eps, n) -> np.ndarray:
+    u = np.array(u, np.complex128, copy=True)
+    lib().orc_flow_steps(_dp(u), _dims(dims), eps, n)
+    return u
+
+
+def staple(u, dims, site, mu) -> np.ndarray:
+    u = np.ascontiguousarray(u, np.complex128)
+    out = np.zeros((3, 3), np.complex128)
+    lib().orc_staple(_dp(u), _dims(dims), site, mu, _dp(out))
+    return out
+
+
+def exp_su3(z, coeff) -> np.ndarray:
+    z = np.ascontiguousarray(z, np.complex128)
+    out = np.zeros((3, 3), np.complex128)
+    lib().orc_exp_su3(_dp(z), coeff, _dp(out))
+    return out
+
+
+def proj_lie(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, np.complex128)
+    out = np.zeros((3, 3), np.complex128)
+    lib().orc_proj_lie(_dp(a), _dp(out))
+    return out
+
+
+def philox(ctr, key):
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    lib().orc_philox(c, k, o)
+    return list(o)
+
+
+def mt19937_64_nth(seed: int, n: int) -> int:
+    return lib().orc_mt19937_64_nth(seed, n)
+
+
+def heatbath_cb(u, dims, beta, n_sweeps, n_hits, seed, sweep_offset=0):
+    """The library's checkerboard/Philox heatbath restated in FP64; returns (links, kp_fails)."""
+    u = np.array(u, np.complex128, copy=True)
+    fails = lib().orc_heatbath_cb(_dp(u), _dims(dims), beta, n_sweeps, n_hits, C.c_uint64(seed),
+                                  C.c_uint64(sweep_offset))
+    return u, int(fails)
+
+
+def gauge_transform_philox(u, dims, seed):
+    u = np.array(u, np.complex128, copy=True)
+    lib().orc_gauge_transform_philox(_dp(u), _dims(dims), C.c_uint64(seed))
+    return u
+
+
+def kp_samples(beta, k, n, seed) -> np.ndarray:
+    out = np.zeros(n)
+    lib().orc_kp_samples(beta, k, n, C.c_uint64(seed), _dp(out))
+    return out
+
+
+class RefChain:
+    """Single-rank reference schedule: frozen links + random shift + lexicographic sweep
+    with std::mt19937_64 (src/bin/gauge_hb_ncb.cpp:18-179)."""
+
+    def __init__(self, L: int, seed: int, cold_start: bool):
+        self.L = L
+        self.h = lib().orc_ref_create(L, seed, 1 if cold_start else 0)
+
+    def run(self, beta, n_shift, n_sweeps=1, n_hits=1) -> np.ndarray:
+        out = np.zeros(n_shift)
+        lib().orc_ref_run(self.h, beta, n_shift, n_sweeps, n_hits, _dp(out))
+        return out
+
+    def sweeps(self, beta, n_sweeps, n_hits=1):
+        lib().orc_ref_sweeps(self.h, beta, n_sweeps, n_hits)
+
+    def links(self) -> np.ndarray:
+        u = np.zeros(shape((self.L,) * 4), np.complex128)
+        lib().orc_ref_get_links(self.h, _dp(u))
+        return u
+
+    def set_links(self, u):
+        u = np.ascontiguousarray(u, np.complex128)
+        lib().orc_ref_set_links(self.h, _dp(u))
+
+    def updates_per_sweep(self) -> int:
+        L = self.L
+        return 4 * L * (L - 1) ** 3
+
+    def __del__(self):
+        try:
+            lib().orc_ref_destroy(self.h)
+        except Exception:
+            pass
+
+
+# ---- ILDG / LIME restatement (src/io/ildg.cpp:13-237) ------------------------------------
+_LIME_MAGIC = 0x456789AB
+
+
+def ildg_xml(dims) -> bytes:
+    """generate_ildg_xml (src/io/ildg.cpp:13-22) with per-axis extents."""
+    lx, ly, lz, lt = dims
+    return ('<?xml version="1.0" encoding="UTF-8"?>\n'
+            '<ildgFormat><version>1.0</version><field>su3gauge</field>'
+            f'<precision>64</precision><lx>{lx}</lx><ly>{ly}</ly><lz>{lz}</lz><lt>{lt}</lt>'
+            '</ildgFormat>').encode()
+
+
+def _lime_header(mb: bool, me: bool, rtype: str, nbytes: int) -> bytes:
+    import struct
+    flags = (0x8000 if mb else 0) | (0x4000 if me else 0)
+    return struct.pack(">IHHQ", _LIME_MAGIC, 1, flags, nbytes) + rtype.encode().ljust(128, b"\0")
+
+
+def write_ildg(path, u, dims) -> None:
+    """LIME file: 'ildg-format' record (MB=1, ME=1), padding, 'ildg-binary-data' header
+    (MB=0, ME=1), then big-endian FP64 links in t, z, y, x, mu, i, j, (re, im) order."""
+    xml = ildg_xml(dims)
+    data = np.ascontiguousarray(u, np.complex128).view(np.float64).astype(">f8").tobytes()
+    with open(path, "wb") as f:
+        f.write(_lime_header(True, True, "ildg-format", len(xml)))
+        f.write(xml)
+        f.write(b"\0" * ((8 - len(xml) % 8) % 8))
+        f.write(_lime_header(False, True, "ildg-binary-data", len(data)))
+        f.write(data)
+
+
+def read_ildg(path, dims) -> np.ndarray:
+    """Scan LIME records for 'ildg-binary-data', check its size, decode big-endian FP64."""
+    import struct
+    raw = open(path, "rb").read()
+    pos = 0
+    expected = int(np.prod(dims)) * 72 * 8
+    while pos + 144 <= len(raw):
+        magic, _ver, _flags, n = struct.unpack(">IHHQ", raw[pos:pos + 16])
+        if magic != _LIME_MAGIC:
+            raise ValueError("bad LIME magic")
+        rtype = raw[pos + 16:pos + 144].split(b"\0")[0].decode()
+        pos += 144
+        if rtype == "ildg-binary-data":
+            if n != expected:
+                raise ValueError("binary data size mismatch")
+            buf = np.frombuffer(raw[pos:pos + n], dtype=">f8").astype(np.float64)
+            if buf.size * 8 != n:
+                raise ValueError("truncated binary data")
+            return buf.view(np.complex128).reshape(shape(dims)).copy()
+        pos += n + (8 - n % 8) % 8
+    raise ValueError("record 'ildg-binary-data' not found")
+
+
+# ---- input-file parser restatement (src/io/io.cpp:290-295, 353-399) -----------------------
+def _stoi(s: str) -> int:
+    import re
+    m = re.match(r"[\s]*([+-]?\d+)", s)
+    if not m:
+        raise ValueError("stoi")
+    v = int(m.group(1))
+    if not -2**31 <= v < 2**31:
+        raise OverflowError("stoi")
+    return v
+
+
+def _stod(s: str) -> float:
+    import re
+    m = re.match(r"[\s]*([+-]?(\d+\.?\d*([eE][+-]?\d+)?|\.\d+([eE][+-]?\d+)?|inf(inity)?|nan))", s, re.I)
+    if not m:
+        raise ValueError("stod")
+    return float(m.group(1))
+
+
+HB_DEFAULTS = dict(L_core=6, n_core_dims=2, cold_start=1, N_switch_eo=3, N_shift=2, seed=123, beta=6.0,
+                   N_samples=10, N_hits=1, N_sweeps=1, N_therm=100, topo=1, N_shift_plaquette=2,
+                   N_shift_topo=10, N_steps_gf=10, N_rk_steps=40, save_each_shifts=2, run_name="c",
+                   run_dir="data")
+
+
+def load_params(path) -> dict:
+    """io::load_params(..., RunParamsHbCB&): returns the parameter dict (defaults from
+    src/io/params.h:46-63); raises ValueError/OverflowError where std::stoi/stod throw."""
+    cfg = {}
+    with open(path, "rb") as f:
+        for raw in f.read().split(b"\n"):
+            line = raw.decode("latin-1")
+            if not line or line[0] == "#":
+                continue
+            if "=" not in line:
+                continue
+            key, value = line.split("=", 1)
+            if value == "":
+                continue
+            cfg[key.strip(" \t")] = value.strip(" \t")
+    p = dict(HB_DEFAULTS)
+    ints = {"L_core": "L_core", "n_core_dims": "n_core_dims", "seed": "seed", "N_shift": "N_shift",
+            "N_sweeps": "N_sweeps", "N_hits": "N_hits", "N_shift_plaquette": "N_shift_plaquette",
+            "N_shift_therm": "N_therm", "N_shift_topo": "N_shift_topo", "N_steps_gf": "N_steps_gf",
+            "N_rk_steps": "N_rk_steps", "save_each_shifts": "save_each_shifts"}
+    for k, dst in ints.items():
+        if k in cfg:
+            p[dst] = _stoi(cfg[k])
+    if "cold_start" in cfg:
+        p["cold_start"] = int(cfg["cold_start"] == "true")
+    if "topo" in cfg:
+        p["topo"] = int(cfg["topo"] == "true")
+    if "beta" in cfg:
+        p["beta"] = _stod(cfg["beta"])
+    p["N_samples"] = 1
+    for k in ("run_name", "run_dir"):
+        if k in cfg:
+            p[k] = cfg[k]
+    return p

@@ -1,0 +1,724 @@
+// qcb_oracle.cpp — FP64 CPU restatement of the ECMC-QNCB heatbath / plaquette / Wilson-flow
+// path.  TEST INFRASTRUCTURE ONLY: it is the checker for the CUDA library, and the timed
+// CPU baseline.  Nothing in the product links or calls it.
+//
+// PARITY UNPINNED: the reference cannot be compiled here (it needs MPI, Eigen3 and c-lime,
+// none of which is installed) and it ships no tests, golden vectors or fixtures.  This
+// restatement follows the reference source line by line (citations below, paths relative
+// to the reference project) and is checked against known answers instead: the C++
+// standard's mt19937_64 known value, the Philox4x32-10 known-answer vectors, scipy's expm,
+// cold-start values and gauge/translation invariance.
+//
+// Field layout: array-of-structures over the periodic lattice without halo, in ILDG order:
+//   links[((s*4 + mu)*9 + i*3 + j)], s = x + Lx*(y + Ly*(z + Lz*t))
+// which is the reference's GaugeField layout (src/gauge/GaugeField.h:27,49-56) with the
+// one-site halo removed.  On a single rank the halo holds copies of the periodic
+// neighbours, and the frozen-link mask guarantees that every halo link read during a sweep
+// is a copy of a frozen link (src/geometry/GeometryCB.cpp:33-56), so periodic indexing
+// reproduces the single-rank reference exactly.
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <complex>
+#include <limits>
+#include <random>
+#include <vector>
+
+namespace orc {
+
+using C = std::complex<double>;
+
+struct M3 {
+  C a[9];
+  C& operator()(int i, int j) { return a[i * 3 + j]; }
+  const C& operator()(int i, int j) const { return a[i * 3 + j]; }
+};
+
+static M3 zero() {
+  M3 m;
+  for (auto& v : m.a) v = 0.0;
+  return m;
+}
+static M3 ident() {
+  M3 m = zero();
+  m(0, 0) = m(1, 1) = m(2, 2) = 1.0;
+  return m;
+}
+static M3 mul(const M3& x, const M3& y) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r(i, j) = x(i, 0) * y(0, j) + x(i, 1) * y(1, j) + x(i, 2) * y(2, j);
+  return r;
+}
+static M3 adj(const M3& x) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r(i, j) = std::conj(x(j, i));
+  return r;
+}
+static M3 add(const M3& x, const M3& y) {
+  M3 r;
+  for (int k = 0; k < 9; ++k) r.a[k] = x.a[k] + y.a[k];
+  return r;
+}
+static M3 sub(const M3& x, const M3& y) {
+  M3 r;
+  for (int k = 0; k < 9; ++k) r.a[k] = x.a[k] - y.a[k];
+  return r;
+}
+static M3 scale(C s, const M3& x) {
+  M3 r;
+  for (int k = 0; k < 9; ++k) r.a[k] = s * x.a[k];
+  return r;
+}
+static C trace(const M3& x) { return x(0, 0) + x(1, 1) + x(2, 2); }
+// Cofactor expansion along the first column.
+static C det(const M3& m) {
+  return m(0, 0) * (m(1, 1) * m(2, 2) - m(1, 2) * m(2, 1)) - m(1, 0) * (m(0, 1) * m(2, 2) - m(0, 2) * m(2, 1)) +
+         m(2, 0) * (m(0, 1) * m(1, 2) - m(0, 2) * m(1, 1));
+}
+static double sqnorm(const M3& m) {
+  double s = 0;
+  for (auto& v : m.a) s += std::norm(v);
+  return s;
+}
+
+struct Lat {
+  int L[4];
+  size_t V;
+  C* u;  // borrowed, 36*V complex
+  size_t idx(int x, int y, int z, int t) const {
+    return (size_t)x + (size_t)L[0] * ((size_t)y + (size_t)L[1] * ((size_t)z + (size_t)L[2] * (size_t)t));
+  }
+  void coords(size_t s, int c[4]) const {
+    c[0] = (int)(s % L[0]);
+    s /= L[0];
+    c[1] = (int)(s % L[1]);
+    s /= L[1];
+    c[2] = (int)(s % L[2]);
+    c[3] = (int)(s / L[2]);
+  }
+  // neighbour of s displaced by d (+1 / -1) in direction mu (periodic)
+  size_t nb(size_t s, int mu, int d) const {
+    int c[4];
+    coords(s, c);
+    c[mu] = (c[mu] + d + L[mu]) % L[mu];
+    return idx(c[0], c[1], c[2], c[3]);
+  }
+  M3 get(size_t s, int mu) const {
+    M3 m;
+    memcpy(m.a, u + (s * 4 + mu) * 9, sizeof m.a);
+    return m;
+  }
+  void set(size_t s, int mu, const M3& m) { memcpy(u + (s * 4 + mu) * 9, m.a, sizeof m.a); }
+};
+
+static Lat make(double* aos, const int dims[4]) {
+  Lat l;
+  for (int d = 0; d < 4; ++d) l.L[d] = dims[d];
+  l.V = (size_t)dims[0] * dims[1] * dims[2] * dims[3];
+  l.u = reinterpret_cast<C*>(aos);
+  return l;
+}
+
+// GaugeField::compute_staple (src/gauge/GaugeField.cpp:74-97)
+static M3 staple(const Lat& f, size_t x, int mu) {
+  M3 st = zero();
+  size_t xmu = f.nb(x, mu, +1);
+  for (int nu = 0; nu < 4; nu++) {
+    if (nu == mu) continue;
+    size_t xnu = f.nb(x, nu, +1);
+    M3 U0 = f.get(xmu, nu), U1 = f.get(xnu, mu), U2 = f.get(x, nu);
+    st = add(st, mul(U0, adj(mul(U2, U1))));
+    size_t xmunu = f.nb(xmu, nu, -1);
+    size_t xmnu = f.nb(x, nu, -1);
+    M3 V0 = f.get(xmunu, nu), V1 = f.get(xmnu, mu), V2 = f.get(xmnu, nu);
+    st = add(st, mul(adj(mul(V1, V0)), V2));
+  }
+  return st;
+}
+
+// mean_plaquette_local (src/observables/observables_mpi.cpp:8-29)
+static double plaquette_sum(const Lat& f) {
+  double sum = 0.0;
+  for (size_t s = 0; s < f.V; ++s)
+    for (int mu = 0; mu < 4; mu++)
+      for (int nu = mu + 1; nu < 4; nu++) {
+        M3 U1 = f.get(s, mu);
+        M3 U2 = f.get(f.nb(s, mu, +1), nu);
+        M3 U3 = adj(f.get(f.nb(s, nu, +1), mu));
+        M3 U4 = adj(f.get(s, nu));
+        sum += trace(mul(mul(mul(U1, U2), U3), U4)).real() / 3.0;
+      }
+  return sum;
+}
+
+// clover_site (observables_mpi.cpp:61-85)
+static M3 clover(const Lat& f, size_t x, int mu, int nu) {
+  size_t xpmu = f.nb(x, mu, +1), xpnu = f.nb(x, nu, +1), xmmu = f.nb(x, mu, -1), xmnu = f.nb(x, nu, -1);
+  size_t xmmupnu = f.nb(xmmu, nu, +1), xmmumnu = f.nb(xmmu, nu, -1), xpmumnu = f.nb(xpmu, nu, -1);
+  M3 c = zero();
+  c = add(c, mul(mul(mul(f.get(x, mu), f.get(xpmu, nu)), adj(f.get(xpnu, mu))), adj(f.get(x, nu))));
+  c = add(c, mul(mul(mul(f.get(x, nu), adj(f.get(xmmupnu, mu))), adj(f.get(xmmu, nu))), f.get(xmmu, mu)));
+  c = add(c, mul(mul(mul(adj(f.get(xmmu, mu)), adj(f.get(xmmumnu, nu))), f.get(xmmumnu, mu)), f.get(xmnu, nu)));
+  c = add(c, mul(mul(mul(adj(f.get(xmnu, nu)), f.get(xmnu, mu)), f.get(xpmumnu, nu)), adj(f.get(x, mu))));
+  M3 F = sub(c, adj(c));
+  return scale(0.125, F);
+}
+
+// local_q_e_clover (observables_mpi.cpp:88-107) and topo_q_e_clover (:110-127)
+static void topo_qe(const Lat& f, double* q_tot, double* e_tot) {
+  double q = 0.0, e = 0.0;
+  for (size_t s = 0; s < f.V; ++s) {
+    M3 F01 = clover(f, s, 0, 1), F02 = clover(f, s, 0, 2), F03 = clover(f, s, 0, 3);
+    M3 F12 = clover(f, s, 1, 2), F13 = clover(f, s, 1, 3), F23 = clover(f, s, 2, 3);
+    double ql = trace(mul(F01, F23)).real() - trace(mul(F02, F13)).real() + trace(mul(F03, F12)).real();
+    double el = 0.5 * (sqnorm(F01) + sqnorm(F02) + sqnorm(F03) + sqnorm(F12) + sqnorm(F13) + sqnorm(F23));
+    q += ql * (1.0 / (4.0 * M_PI * M_PI));
+    e += el;
+  }
+  *q_tot = q;
+  *e_tot = e;
+}
+
+// proj_lie_su3 (src/su3/utils.cpp:130-134)
+static void proj_lie(M3& A) {
+  M3 B = scale(0.5, sub(A, adj(A)));
+  C tr = trace(B) / 3.0;
+  A = sub(B, scale(tr, ident()));
+}
+
+// exp_su3_luscher (src/su3/utils.cpp:145-193)
+static M3 exp_luscher(const M3& Z, double coeff) {
+  const C I(0.0, 1.0);
+  M3 X = scale(coeff, Z);
+  M3 X2 = mul(X, X);
+  double t = -0.5 * trace(X2).real();
+  double d = (I * det(X)).real();
+  const int N = 18;
+  double c[N + 1];
+  c[0] = 1.0;
+  for (int n = 1; n <= N; ++n) c[n] = c[n - 1] / (double)n;
+  C q0 = c[N], q1 = 0.0, q2 = 0.0;
+  for (int n = N - 1; n >= 0; --n) {
+    C q0n = c[n] - I * d * q2;
+    C q1n = q0 - t * q2;
+    C q2n = q1;
+    q0 = q0n;
+    q1 = q1n;
+    q2 = q2n;
+  }
+  return add(add(scale(q0, ident()), scale(q1, X)), scale(q2, X2));
+}
+
+// GradientFlow (src/flow/gradient_flow.cpp:10-128) on a lattice without halo.
+struct Flow {
+  Lat* f;
+  double eps;
+  std::vector<C> f0, f1;  // force_0, force_1
+  void force(std::vector<C>& out) {  // compute_force (:15-34)
+    for (size_t s = 0; s < f->V; ++s)
+      for (int mu = 0; mu < 4; ++mu) {
+        M3 st = staple(*f, s, mu);
+        M3 tmp = mul(scale(-1.0, f->get(s, mu)), st);
+        proj_lie(tmp);
+        memcpy(&out[(s * 4 + mu) * 9], tmp.a, sizeof tmp.a);
+      }
+  }
+  M3 at(const std::vector<C>& v, size_t s, int mu) const {
+    M3 m;
+    memcpy(m.a, &v[(s * 4 + mu) * 9], sizeof m.a);
+    return m;
+  }
+  void rk3_step() {  // rk3_step (:117-128)
+    f0.resize(f->V * 36);
+    f1.resize(f->V * 36);
+    force(f0);
+    for (size_t s = 0; s < f->V; ++s)  // compute_w1 (:37-53)
+      for (int mu = 0; mu < 4; ++mu) f->set(s, mu, mul(exp_luscher(at(f0, s, mu), 0.25 * eps), f->get(s, mu)));
+    force(f1);
+    for (size_t s = 0; s < f->V; ++s)  // compute_w2 (:56-74)
+      for (int mu = 0; mu < 4; ++mu) {
+        M3 Z = sub(scale((8.0 / 9.0) * eps, at(f1, s, mu)), scale((17.0 / 36.0) * eps, at(f0, s, mu)));
+        f->set(s, mu, mul(exp_luscher(Z, 1.0), f->get(s, mu)));
+      }
+    for (size_t s = 0; s < f->V; ++s)  // replace_force_0 (:77-93)
+      for (int mu = 0; mu < 4; ++mu) {
+        M3 tmp = sub(scale(8.0 / 9.0, at(f1, s, mu)), scale(17.0 / 36.0, at(f0, s, mu)));
+        memcpy(&f0[(s * 4 + mu) * 9], tmp.a, sizeof tmp.a);
+      }
+    force(f1);
+    for (size_t s = 0; s < f->V; ++s)  // compute_w3 (:96-114)
+      for (int mu = 0; mu < 4; ++mu) {
+        M3 Z = sub(scale(0.75 * eps, at(f1, s, mu)), scale(eps, at(f0, s, mu)));
+        f->set(s, mu, mul(exp_luscher(Z, 1.0), f->get(s, mu)));
+      }
+  }
+};
+
+// ---- SU(2) helpers (src/su3/utils.cpp:33-63) -----------------------------------------
+struct Q4 {
+  double v[4];
+};
+static M3 su2_quaternion_to_su3(const Q4& q, int i, int j) {
+  M3 X = zero();
+  int k = 3 - i - j;
+  X(k, k) = 1.0;
+  X(i, i) = C(q.v[0], q.v[3]);
+  X(j, j) = C(q.v[0], -q.v[3]);
+  X(i, j) = C(q.v[2], q.v[1]);
+  X(j, i) = C(-q.v[2], q.v[1]);
+  return X;
+}
+// quaternion of the 2x2 block [[w00, w01], [w10, w11]]
+static Q4 su2_to_quaternion(C w00, C w01, C w10, C w11) {
+  return {{(w00 + w11).real() / 2.0, (w01 + w10).imag() / 2.0, (w01 - w10).real() / 2.0, (w00 - w11).imag() / 2.0}};
+}
+static Q4 qmult(const Q4& q, const Q4& p) {
+  return {{q.v[0] * p.v[0] - q.v[1] * p.v[1] - q.v[2] * p.v[2] - q.v[3] * p.v[3],
+           q.v[0] * p.v[1] + q.v[1] * p.v[0] + q.v[2] * p.v[3] - q.v[3] * p.v[2],
+           q.v[0] * p.v[2] - q.v[1] * p.v[3] + q.v[2] * p.v[0] + q.v[3] * p.v[1],
+           q.v[0] * p.v[3] + q.v[1] * p.v[2] - q.v[2] * p.v[1] + q.v[3] * p.v[0]}};
+}
+static Q4 qadj(const Q4& q) { return {{q.v[0], -q.v[1], -q.v[2], -q.v[3]}}; }
+
+// ---- reference heatbath with std::mt19937_64 (src/heatbath/heatbath.cpp:8-44) ----------
+static Q4 generate_su2_kp(double beta, double k, std::mt19937_64& rng) {
+  std::uniform_real_distribution<double> dist(0, 1);
+  double alpha = beta * k * 2.0 / 3.0;
+  double a0;
+  while (true) {
+    double delta = dist(rng);
+    double r1 = dist(rng);
+    double r2 = dist(rng);
+    double r3 = dist(rng);
+    double lambda_sq = -0.5 / alpha * (log(r1) + pow(cos(2 * M_PI * r2), 2) * log(r3));
+    if (delta * delta <= 1.0 - lambda_sq) {
+      a0 = 1.0 - 2.0 * lambda_sq;
+      break;
+    }
+  }
+  double r_spatial = sqrt(1.0 - a0 * a0);
+  double phi = 2.0 * M_PI * dist(rng);
+  double cos_theta = 2.0 * dist(rng) - 1.0;
+  double sin_theta = sqrt(1.0 - cos_theta * cos_theta);
+  return {{a0, r_spatial * sin_theta * cos(phi), r_spatial * sin_theta * sin(phi), r_spatial * cos_theta}};
+}
+static Q4 su2_step(double beta, const Q4& w, std::mt19937_64& rng) {
+  double k = sqrt(w.v[0] * w.v[0] + w.v[1] * w.v[1] + w.v[2] * w.v[2] + w.v[3] * w.v[3]);
+  Q4 v = {{w.v[0] / k, w.v[1] / k, w.v[2] / k, w.v[3] / k}};
+  Q4 x = generate_su2_kp(beta, k, rng);
+  return qmult(x, qadj(v));
+}
+// mpi::heatbathcb::hit (src/heatbath/heatbath_mpi.cpp:11-34)
+static void hit_ref(Lat& f, size_t s, int mu, double beta, std::mt19937_64& rng) {
+  M3 A = staple(f, s, mu);
+  const int sub[3][2] = {{0, 1}, {1, 2}, {0, 2}};
+  for (int g = 0; g < 3; ++g) {
+    int i = sub[g][0], j = sub[g][1];
+    M3 W = mul(f.get(s, mu), A);
+    Q4 wq = su2_to_quaternion(W(i, i), W(i, j), W(j, i), W(j, j));
+    Q4 r = su2_step(beta, wq, rng);
+    f.set(s, mu, mul(su2_quaternion_to_su3(r, i, j), f.get(s, mu)));
+  }
+}
+
+// Frozen links on one rank (src/geometry/GeometryCB.cpp:33-56): link (c, mu) with
+// c_d == 1 (1-based, i.e. 0 here) for some d != mu.
+static bool frozen(const int c[4], int mu) {
+  for (int d = 0; d < 4; ++d)
+    if (d != mu && c[d] == 0) return true;
+  return false;
+}
+
+// mpi::heatbathcb::sweep (heatbath_mpi.cpp:37-56): lexicographic t, z, y, x, mu order.
+static void sweep_ref(Lat& f, double beta, int n_hits, std::mt19937_64& rng) {
+  for (size_t s = 0; s < f.V; ++s) {
+    int c[4];
+    f.coords(s, c);
+    for (int mu = 0; mu < 4; ++mu)
+      if (!frozen(c, mu))
+        for (int h = 0; h < n_hits; ++h) hit_ref(f, s, mu, beta, rng);
+  }
+}
+
+// mpi::shift::random_shift on one rank (src/mpi/Shift.cpp:109-186):
+// new(c) = old(c - s), periodic, with s drawn in x, y, z, t order.
+static void random_shift(Lat& f, std::mt19937_64& rng, std::vector<C>& tmp) {
+  std::uniform_int_distribution<int> rand_l_shift(0, f.L[0] - 1);
+  int sh[4];
+  sh[0] = rand_l_shift(rng);
+  sh[1] = rand_l_shift(rng);
+  sh[2] = rand_l_shift(rng);
+  sh[3] = rand_l_shift(rng);
+  tmp.assign(f.u, f.u + f.V * 36);
+  for (size_t s = 0; s < f.V; ++s) {
+    int c[4];
+    f.coords(s, c);
+    int o[4];
+    for (int d = 0; d < 4; ++d) o[d] = ((c[d] - sh[d]) % f.L[d] + f.L[d]) % f.L[d];
+    size_t so = f.idx(o[0], o[1], o[2], o[3]);
+    memcpy(f.u + s * 36, &tmp[so * 36], 36 * sizeof(C));
+  }
+}
+
+// random_su3 (src/su3/utils.cpp:13-30): complex Gaussian 3x3, Householder QR (LAPACK /
+// Eigen convention: beta = -sign(Re c0) |x|, tau = conj((beta - c0)/beta), Q = H0^* H1^* H2^*),
+// then Q / det(Q)^(1/3).
+static M3 random_su3_ref(std::mt19937_64& rng) {
+  std::normal_distribution<double> gauss(0.0, 1.0);
+  M3 z;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) z(i, j) = C(gauss(rng), gauss(rng));
+  C tau[3];
+  M3 a = z;
+  for (int k = 0; k < 3; ++k) {
+    double tail = 0.0;
+    for (int i = k + 1; i < 3; ++i) tail += std::norm(a(i, k));
+    C c0 = a(k, k);
+    const double tol = std::numeric_limits<double>::min();
+    double beta;
+    if (tail <= tol && std::norm(c0.imag()) <= tol) {
+      tau[k] = 0.0;
+      beta = c0.real();
+      for (int i = k + 1; i < 3; ++i) a(i, k) = 0.0;
+    } else {
+      beta = sqrt(std::norm(c0) + tail);
+      if (c0.real() >= 0.0) beta = -beta;
+      for (int i = k + 1; i < 3; ++i) a(i, k) = a(i, k) / (c0 - beta);
+      tau[k] = std::conj((beta - c0) / beta);
+    }
+    a(k, k) = beta;
+    // apply (I - tau v v^*) to the trailing columns, v = [1, a(k+1..,k)]
+    for (int j = k + 1; j < 3; ++j) {
+      C w = a(k, j);
+      for (int i = k + 1; i < 3; ++i) w += std::conj(a(i, k)) * a(i, j);
+      a(k, j) -= tau[k] * w;
+      for (int i = k + 1; i < 3; ++i) a(i, j) -= tau[k] * a(i, k) * w;
+    }
+  }
+  // Q = G0 G1 G2 with G_k = I - conj(tau_k) v_k v_k^*, accumulated from the right.
+  M3 Q = ident();
+  for (int k = 2; k >= 0; --k) {
+    C h = std::conj(tau[k]);
+    for (int j = 0; j < 3; ++j) {
+      C w = Q(k, j);
+      for (int i = k + 1; i < 3; ++i) w += std::conj(a(i, k)) * Q(i, j);
+      Q(k, j) -= h * w;
+      for (int i = k + 1; i < 3; ++i) Q(i, j) -= h * a(i, k) * w;
+    }
+  }
+  C dq = det(Q);
+  C root = std::pow(dq, 1.0 / 3.0);
+  return scale(1.0 / root, Q);
+}
+
+// ---- Philox4x32-10 (Salmon et al., SC'11) and the library's checkerboard heatbath -----
+struct P4 {
+  uint32_t v[4];
+};
+static P4 philox(P4 c, uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c.v[0];
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c.v[2];
+    P4 n;
+    n.v[0] = (uint32_t)(p1 >> 32) ^ c.v[1] ^ k0;
+    n.v[1] = (uint32_t)p1;
+    n.v[2] = (uint32_t)(p0 >> 32) ^ c.v[3] ^ k1;
+    n.v[3] = (uint32_t)p0;
+    c = n;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+static double u01(uint32_t w) { return ((double)w + 0.5) * 2.3283064365386963e-10; }
+
+static const uint32_t KP_CAP = 4096;
+
+// One subgroup update with Philox draws keyed (link, sweep, hsg, attempt); same
+// arithmetic as the reference su2_step / generate_su2_kp.  Returns false at the cap.
+static bool cb_subgroup(M3& U, const M3& A, int i, int j, double beta, uint32_t link, uint32_t sweep, uint32_t hsg,
+                        uint32_t k0, uint32_t k1) {
+  M3 W = mul(U, A);
+  Q4 w = su2_to_quaternion(W(i, i), W(i, j), W(j, i), W(j, j));
+  double k = sqrt(w.v[0] * w.v[0] + w.v[1] * w.v[1] + w.v[2] * w.v[2] + w.v[3] * w.v[3]);
+  Q4 v = {{w.v[0] / k, w.v[1] / k, w.v[2] / k, w.v[3] / k}};
+  double alpha = beta * k * 2.0 / 3.0;
+  double a0 = 0;
+  bool ok = false;
+  for (uint32_t att = 0; att < KP_CAP; ++att) {
+    P4 r = philox({{link, sweep, hsg, att}}, k0, k1);
+    double delta = u01(r.v[0]), r1 = u01(r.v[1]), r2 = u01(r.v[2]), r3 = u01(r.v[3]);
+    double cs = cos(2 * M_PI * r2);
+    double lambda_sq = -0.5 / alpha * (log(r1) + cs * cs * log(r3));
+    if (delta * delta <= 1.0 - lambda_sq) {
+      a0 = 1.0 - 2.0 * lambda_sq;
+      ok = true;
+      break;
+    }
+  }
+  if (!ok) return false;
+  P4 r = philox({{link, sweep, hsg, 0xFFFFFFFFu}}, k0, k1);
+  double phi = 2.0 * M_PI * u01(r.v[0]);
+  double cos_theta = 2.0 * u01(r.v[1]) - 1.0;
+  double sin_theta = sqrt(std::max(0.0, 1.0 - cos_theta * cos_theta));
+  double rs = sqrt(std::max(0.0, 1.0 - a0 * a0));
+  Q4 x = {{a0, rs * sin_theta * cos(phi), rs * sin_theta * sin(phi), rs * cos_theta}};
+  Q4 q = qmult(x, qadj(v));
+  U = mul(su2_quaternion_to_su3(q, i, j), U);
+  return true;
+}
+
+static uint64_t heatbath_cb(Lat& f, double beta, int n_sweeps, int n_hits, uint64_t seed, uint64_t sweep_offset) {
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  uint64_t fails = 0;
+  for (int sw = 0; sw < n_sweeps; ++sw) {
+    const uint32_t sweep = (uint32_t)(sweep_offset + (uint64_t)sw);
+    for (int mu = 0; mu < 4; ++mu)
+      for (int par = 0; par < 2; ++par)
+        for (size_t s = 0; s < f.V; ++s) {
+          int c[4];
+          f.coords(s, c);
+          if (((c[0] + c[1] + c[2] + c[3]) & 1) != par) continue;
+          M3 A = staple(f, s, mu);
+          M3 U = f.get(s, mu);
+          const uint32_t link = (uint32_t)mu * (uint32_t)f.V + (uint32_t)s;
+          for (int h = 0; h < n_hits; ++h) {
+            const uint32_t hb = (uint32_t)h << 2;
+            fails += !cb_subgroup(U, A, 0, 1, beta, link, sweep, hb | 0u, k0, k1);
+            fails += !cb_subgroup(U, A, 1, 2, beta, link, sweep, hb | 1u, k0, k1);
+            fails += !cb_subgroup(U, A, 0, 2, beta, link, sweep, hb | 2u, k0, k1);
+          }
+          f.set(s, mu, U);
+        }
+  }
+  return fails;
+}
+
+// Haar SU(3) from the Philox stream: rows 0, 1 complex Gaussian (Box-Muller), Gram-Schmidt,
+// row 2 = conj(row0 x row1).
+static M3 haar_philox(uint32_t id, uint32_t tag, uint32_t k0, uint32_t k1) {
+  double n[12];
+  for (int call = 0; call < 3; ++call) {
+    P4 r = philox({{id, 0u, tag, (uint32_t)call}}, k0, k1);
+    for (int pr = 0; pr < 2; ++pr) {
+      double u1 = u01(r.v[2 * pr]), u2 = u01(r.v[2 * pr + 1]);
+      double rad = sqrt(-2.0 * log(u1));
+      n[call * 4 + pr * 2 + 0] = rad * cos(2 * M_PI * u2);
+      n[call * 4 + pr * 2 + 1] = rad * sin(2 * M_PI * u2);
+    }
+  }
+  C r0[3], r1[3];
+  for (int j = 0; j < 3; ++j) {
+    r0[j] = C(n[2 * j], n[2 * j + 1]);
+    r1[j] = C(n[6 + 2 * j], n[6 + 2 * j + 1]);
+  }
+  double n0 = std::norm(r0[0]) + std::norm(r0[1]) + std::norm(r0[2]);
+  for (auto& v : r0) v /= sqrt(n0);
+  C d = std::conj(r0[0]) * r1[0] + std::conj(r0[1]) * r1[1] + std::conj(r0[2]) * r1[2];
+  for (int j = 0; j < 3; ++j) r1[j] -= d * r0[j];
+  double n1 = std::norm(r1[0]) + std::norm(r1[1]) + std::norm(r1[2]);
+  for (auto& v : r1) v /= sqrt(n1);
+  M3 u;
+  for (int j = 0; j < 3; ++j) {
+    u(0, j) = r0[j];
+    u(1, j) = r1[j];
+  }
+  u(2, 0) = std::conj(r0[1] * r1[2] - r0[2] * r1[1]);
+  u(2, 1) = std::conj(r0[2] * r1[0] - r0[0] * r1[2]);
+  u(2, 2) = std::conj(r0[0] * r1[1] - r0[1] * r1[0]);
+  return u;
+}
+
+const uint32_t DOMAIN_HOT = 0x80000000u, DOMAIN_GAUGE = 0x90000000u;
+
+// Reference-schedule chain state (one rank): lattice + mt19937_64.
+struct RefChain {
+  int dims[4];
+  std::vector<C> links;
+  std::mt19937_64 rng;
+  std::vector<C> tmp;
+  Lat lat() {
+    Lat l;
+    for (int d = 0; d < 4; ++d) l.L[d] = dims[d];
+    l.V = (size_t)dims[0] * dims[1] * dims[2] * dims[3];
+    l.u = links.data();
+    return l;
+  }
+};
+
+}  // namespace orc
+
+using namespace orc;
+
+extern "C" {
+
+int orc_plaquette(const double* aos, const int dims[4], double* out) {
+  Lat f = make(const_cast<double*>(aos), dims);
+  *out = plaquette_sum(f) / (6.0 * (double)f.V);
+  return 0;
+}
+
+int orc_topo_qe(const double* aos, const int dims[4], double* q, double* e) {
+  Lat f = make(const_cast<double*>(aos), dims);
+  double qt, et;
+  topo_qe(f, &qt, &et);
+  *q = qt;
+  *e = et / (double)f.V;
+  return 0;
+}
+
+// topo_charge_flowed (observables_mpi.cpp:153-178) on a copy of aos.
+int orc_flow_measure(const double* aos, const int dims[4], double eps, int n_steps_gf, int n_rk_steps, double* tQE) {
+  size_t V = (size_t)dims[0] * dims[1] * dims[2] * dims[3];
+  std::vector<double> copy(aos, aos + V * 72);
+  Lat f = make(copy.data(), dims);
+  Flow gf{&f, eps, {}, {}};
+  double t = 0.0;
+  for (int st = 0; st < n_steps_gf; st++) {
+    double q, e;
+    topo_qe(f, &q, &e);
+    tQE[3 * st] = t;
+    tQE[3 * st + 1] = q;
+    tQE[3 * st + 2] = e / (double)V;
+    for (int r = 0; r < n_rk_steps; r++) {
+      gf.rk3_step();
+      t += eps;
+    }
+  }
+  return 0;
+}
+
+int orc_flow_steps(double* aos, const int dims[4], double eps, int n) {
+  Lat f = make(aos, dims);
+  Flow gf{&f, eps, {}, {}};
+  for (int r = 0; r < n; ++r) gf.rk3_step();
+  return 0;
+}
+
+int orc_staple(const double* aos, const int dims[4], long site, int mu, double* out18) {
+  Lat f = make(const_cast<double*>(aos), dims);
+  M3 a = staple(f, (size_t)site, mu);
+  memcpy(out18, a.a, sizeof a.a);
+  return 0;
+}
+
+int orc_exp_su3(const double* z18, double coeff, double* out18) {
+  M3 z;
+  memcpy(z.a, z18, sizeof z.a);
+  M3 r = exp_luscher(z, coeff);
+  memcpy(out18, r.a, sizeof r.a);
+  return 0;
+}
+
+int orc_proj_lie(const double* a18, double* out18) {
+  M3 a;
+  memcpy(a.a, a18, sizeof a.a);
+  proj_lie(a);
+  memcpy(out18, a.a, sizeof a.a);
+  return 0;
+}
+
+int orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  P4 r = philox({{ctr[0], ctr[1], ctr[2], ctr[3]}}, key[0], key[1]);
+  memcpy(out, r.v, sizeof r.v);
+  return 0;
+}
+
+uint64_t orc_mt19937_64_nth(uint64_t seed, int n) {
+  std::mt19937_64 g(seed);
+  uint64_t v = 0;
+  for (int k = 0; k < n; ++k) v = g();
+  return v;
+}
+
+// Library schedule (checkerboard, Philox) restated in FP64; returns KP cap hits.
+uint64_t orc_heatbath_cb(double* aos, const int dims[4], double beta, int n_sweeps, int n_hits, uint64_t seed,
+                         uint64_t sweep_offset) {
+  Lat f = make(aos, dims);
+  return heatbath_cb(f, beta, n_sweeps, n_hits, seed, sweep_offset);
+}
+
+int orc_hot_start_philox(double* aos, const int dims[4], uint64_t seed) {
+  Lat f = make(aos, dims);
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  for (size_t s = 0; s < f.V; ++s)
+    for (int mu = 0; mu < 4; ++mu) f.set(s, mu, haar_philox((uint32_t)mu * (uint32_t)f.V + (uint32_t)s, DOMAIN_HOT, k0, k1));
+  return 0;
+}
+
+int orc_gauge_transform_philox(double* aos, const int dims[4], uint64_t seed) {
+  Lat f = make(aos, dims);
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  std::vector<C> out(f.V * 36);
+  for (size_t s = 0; s < f.V; ++s)
+    for (int mu = 0; mu < 4; ++mu) {
+      M3 G = haar_philox((uint32_t)s, DOMAIN_GAUGE, k0, k1);
+      M3 Gy = haar_philox((uint32_t)f.nb(s, mu, +1), DOMAIN_GAUGE, k0, k1);
+      M3 r = mul(mul(G, f.get(s, mu)), adj(Gy));
+      memcpy(&out[(s * 4 + mu) * 9], r.a, sizeof r.a);
+    }
+  memcpy(f.u, out.data(), out.size() * sizeof(C));
+  return 0;
+}
+
+// Kennedy-Pendleton sampler of the reference with mt19937_64 (for distribution tests).
+int orc_kp_samples(double beta, double k, int n, uint64_t seed, double* a0) {
+  std::mt19937_64 rng(seed);
+  for (int i = 0; i < n; ++i) a0[i] = generate_su2_kp(beta, k, rng).v[0];
+  return 0;
+}
+
+// ---- reference-schedule chain (frozen links + random shift, mt19937_64) ---------------
+// generate_hb_cb (src/bin/gauge_hb_ncb.cpp:18-179) for one rank (n_core_dims = 1).
+void* orc_ref_create(int L, int seed, int cold_start) {
+  RefChain* c = new RefChain();
+  for (int d = 0; d < 4; ++d) c->dims[d] = L;
+  size_t V = (size_t)L * L * L * L;
+  c->links.assign(V * 36, C(0.0, 0.0));
+  c->rng.seed((uint64_t)(int64_t)seed + 0);  // rp.seed + topo.rank
+  Lat f = c->lat();
+  for (size_t s = 0; s < V; ++s)
+    for (int mu = 0; mu < 4; ++mu) f.set(s, mu, ident());
+  if (!cold_start)  // GaugeField::hot_start (GaugeField.cpp:10-20), t, z, y, x, mu order
+    for (size_t s = 0; s < V; ++s)
+      for (int mu = 0; mu < 4; ++mu) f.set(s, mu, random_su3_ref(c->rng));
+  return c;
+}
+
+void orc_ref_destroy(void* h) { delete static_cast<RefChain*>(h); }
+
+// n_shift iterations of: random_shift, N_sweeps sweeps, plaquette -> plaq[i].
+int orc_ref_run(void* h, double beta, int n_shift, int n_sweeps, int n_hits, double* plaq) {
+  RefChain* c = static_cast<RefChain*>(h);
+  Lat f = c->lat();
+  for (int i = 0; i < n_shift; ++i) {
+    random_shift(f, c->rng, c->tmp);
+    for (int s = 0; s < n_sweeps; ++s) sweep_ref(f, beta, n_hits, c->rng);
+    if (plaq) plaq[i] = plaquette_sum(f) / (6.0 * (double)f.V);
+  }
+  return 0;
+}
+
+// Sweeps only (no shift, no measurement): for timing the reference update rate.
+int orc_ref_sweeps(void* h, double beta, int n_sweeps, int n_hits) {
+  RefChain* c = static_cast<RefChain*>(h);
+  Lat f = c->lat();
+  for (int s = 0; s < n_sweeps; ++s) sweep_ref(f, beta, n_hits, c->rng);
+  return 0;
+}
+
+int orc_ref_get_links(void* h, double* aos) {
+  RefChain* c = static_cast<RefChain*>(h);
+  memcpy(aos, c->links.data(), c->links.size() * sizeof(C));
+  return 0;
+}
+int orc_ref_set_links(void* h, const double* aos) {
+  RefChain* c = static_cast<RefChain*>(h);
+  memcpy(c->links.data(), aos, c->links.size() * sizeof(C));
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,154 @@
+"""CPU tests of libqcb.so's host side: exported symbols, error paths without a GPU, the
+input-file parser and the ILDG container probe (no kernel launches)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+import oracle
+import qcb
+from qcb import _lib
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names |= set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\**\s*(qcb_[a-z_0-9]+)\s*\(", text, flags=re.M))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    names = declared_symbols()
+    assert len(names) >= 25
+    missing = [n for n in sorted(names) if not hasattr(L, n)]
+    assert not missing, missing
+    # and the Python binding declares them all
+    assert names <= set(_lib.SIGNATURES), sorted(names - set(_lib.SIGNATURES))
+
+
+def test_abi_version():
+    assert _lib.lib().qcb_abi_version() == 1
+
+
+def test_null_arguments_are_rejected():
+    L = _lib.lib()
+    assert L.qcb_ctx_create(0, 0, None) == 1
+    assert b"null" in L.qcb_last_error()
+    assert L.qcb_plaquette(None, None) == 1
+    assert L.qcb_heatbath(None, 6.0, 1, 1, 0, 0) == 1
+
+
+def test_context_creation_without_gpu_fails_cleanly():
+    if qcb.device_count() > 0:
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(qcb.QcbError) as e:
+        qcb.Context(0)
+    assert e.value.code == 2
+    assert "CUDA" in str(e.value) or "device" in str(e.value)
+
+
+QUIRKY = """# comment
+L_core=8
+n_core_dims = 1
+cold_start=hot
+seed = 1234 trailing
+N_shift=200
+N_switch_eo=1
+beta = 6.0
+\tN_sweeps\t=\t1
+N_hits = 1
+N_shift_plaquette = 1
+N_shift_therm = 0
+topo = true
+N_shift_topo = 1
+N_steps_gf = 50
+N_rk_steps = 1
+run_name = cfg1
+run_dir = data
+save_each_shifts =
+no_equals_line
+# last one wins
+N_hits = 2
+"""
+
+
+def write(tmp_path, text, name="in.txt"):
+    p = tmp_path / name
+    p.write_bytes(text.encode())
+    return p
+
+
+def test_params_match_reference_semantics(tmp_path):
+    p = write(tmp_path, QUIRKY)
+    got = qcb.io.load_params(p).as_dict()
+    ref = oracle.load_params(p)
+    for k, v in ref.items():
+        assert got[k] == v, (k, got[k], v)
+    assert got["cold_start"] == 0          # "hot" is not "true"
+    assert got["N_hits"] == 2              # later keys override
+    assert got["save_each_shifts"] == 2    # empty value: default kept
+    assert got["N_samples"] == 1           # forced (io.cpp:381)
+    assert got["seed"] == 1234             # std::stoi ignores trailing text
+
+
+def test_params_defaults_and_crlf(tmp_path):
+    p = write(tmp_path, "cold_start=true\r\nbeta=5.7\r\n")
+    got = qcb.io.load_params(p).as_dict()
+    ref = oracle.load_params(p)
+    assert got["cold_start"] == ref["cold_start"] == 0   # trailing \r is not trimmed
+    assert got["beta"] == ref["beta"] == 5.7
+    assert got["N_therm"] == 100 and got["topo"] == 1    # params.h defaults
+
+
+def test_params_errors(tmp_path):
+    with pytest.raises(qcb.QcbError) as e:
+        qcb.io.load_params(tmp_path / "missing.txt")
+    assert e.value.code == 3
+    p = write(tmp_path, "L_core = eight\n")
+    with pytest.raises(qcb.QcbError) as e:
+        qcb.io.load_params(p)
+    assert e.value.code == 4
+    with pytest.raises(ValueError):
+        oracle.load_params(p)
+
+
+def test_reference_example_inputs_parse(tmp_path):
+    # the reference's inputs/hcold6.txt keys, restated
+    text = ("#Lattice params\nL_core=4\nn_core_dims=2\ncold_start=true\n\n#Run params\nseed=12345\n"
+            "N_shift_therm = 0\nN_shift=50000\n\n#Heatbath params\nbeta = 6.0\nN_sweeps = 2\nN_hits = 1\n\n"
+            "#Plaquette params\nN_shift_plaquette = 1\n\n#Topo params\ntopo = false\nN_shift_topo = 25\n"
+            "N_steps_gf = 10\nN_rk_steps = 40\n\n#Save params\nrun_name = hcold62\nrun_dir = data\n"
+            "save_each_shifts = 2000\n")
+    p = write(tmp_path, text)
+    got = qcb.io.load_params(p).as_dict()
+    assert got == {**got, **{k: v for k, v in oracle.load_params(p).items()}}
+    assert got["topo"] == 0 and got["N_sweeps"] == 2 and got["run_name"] == "hcold62"
+
+
+def test_ildg_probe(tmp_path):
+    dims = (4, 4, 4, 4)
+    u = oracle.cold(dims)
+    p = tmp_path / "conf"
+    oracle.write_ildg(p, u, dims)
+    off, n = qcb.io.ildg_probe(p)
+    assert n == 256 * 72 * 8
+    xml = oracle.ildg_xml(dims)
+    assert off == 144 + len(xml) + (8 - len(xml) % 8) % 8 + 144
+    # truncated header and bad magic are format errors
+    raw = p.read_bytes()
+    (tmp_path / "bad").write_bytes(b"\0" * 200)
+    with pytest.raises(qcb.QcbError) as e:
+        qcb.io.ildg_probe(tmp_path / "bad")
+    assert e.value.code == 4
+    (tmp_path / "short").write_bytes(raw[:100])
+    with pytest.raises(qcb.QcbError) as e:
+        qcb.io.ildg_probe(tmp_path / "short")
+    assert e.value.code == 4
+    with pytest.raises(qcb.QcbError) as e:
+        qcb.io.ildg_probe(tmp_path / "nope")
+    assert e.value.code == 3
