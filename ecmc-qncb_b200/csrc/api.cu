@@ -359,8 +359,10 @@ int qcb_gauge_transform(qcb_lattice* L, uint64_t seed) {
 
 }  // extern "C"
 
-// ---- AoS transfers (host <-> device in t-slabs through two staging buffers) ------------
+// ---- AoS transfers (host <-> device in site chunks through two staging buffers) ------
 namespace {
+constexpr uint32_t STAGE_SITES = (uint32_t)(STAGE_BYTES / (72 * sizeof(double)));
+
 int ensure_stage(qcb_ctx* c) {
   if (c->d_stage[0]) return QCB_OK;
   if (cudaMalloc(&c->d_stage[0], STAGE_BYTES) != cudaSuccess ||
@@ -374,29 +376,28 @@ int ensure_stage(qcb_ctx* c) {
   return QCB_OK;
 }
 
-int slab_t(const Geom& g) {
-  const size_t per_t = (size_t)g.str[3] * 72 * sizeof(double);
-  size_t nt = STAGE_BYTES / per_t;
-  if (nt < 1) nt = 1;
-  if (nt > (size_t)g.L[3]) nt = g.L[3];
-  return (int)nt;
+int ensure_host_stage(qcb_ctx* c) {
+  if (c->h_stage) return QCB_OK;
+  if (cudaMallocHost(&c->h_stage, STAGE_BYTES) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(QCB_ERR_NOMEM, "cannot allocate pinned staging buffer");
+  }
+  return QCB_OK;
 }
 
-// host -> device; `host` holds the whole lattice (72*V doubles).
+// host -> device; `host` holds the whole lattice (72*V doubles).  Copies and conversions of
+// consecutive chunks alternate between the two device staging buffers (stream-ordered).
 int upload_aos(qcb_lattice* L, const double* host, int bswap) {
   qcb_ctx* c = L->ctx;
   TRY(ensure_stage(c));
-  const Geom& g = L->dev.g;
-  const size_t per_t = (size_t)g.str[3] * 72;
-  if (per_t * sizeof(double) > STAGE_BYTES) return fail(QCB_ERR_INVALID, "time slice exceeds staging buffer");
-  const int nt = slab_t(g);
+  const uint32_t V = L->dev.g.V;
   int k = 0;
-  for (int t0 = 0; t0 < g.L[3]; t0 += nt, k ^= 1) {
-    const int n = (t0 + nt <= g.L[3]) ? nt : g.L[3] - t0;
-    CU(cudaMemcpyAsync(c->d_stage[k], host + (size_t)t0 * per_t, (size_t)n * per_t * sizeof(double),
+  for (uint32_t s0 = 0; s0 < V; s0 += STAGE_SITES, k ^= 1) {
+    const uint32_t n = (V - s0 < STAGE_SITES) ? V - s0 : STAGE_SITES;
+    CU(cudaMemcpyAsync(c->d_stage[k], host + (size_t)s0 * 72, (size_t)n * 72 * sizeof(double),
                        cudaMemcpyHostToDevice, c->stream),
        "H2D copy");
-    CU(launch_aos_to_soa(L->dev, c->d_stage[k], t0, n, bswap, c->stream, 0), "AoS->SoA");
+    CU(launch_aos_to_soa(L->dev, c->d_stage[k], s0, n, bswap, c->stream, 0), "AoS->SoA");
     c->launches++;
   }
   return QCB_OK;
@@ -405,16 +406,13 @@ int upload_aos(qcb_lattice* L, const double* host, int bswap) {
 int download_aos(qcb_lattice* L, double* host, int bswap) {
   qcb_ctx* c = L->ctx;
   TRY(ensure_stage(c));
-  const Geom& g = L->dev.g;
-  const size_t per_t = (size_t)g.str[3] * 72;
-  if (per_t * sizeof(double) > STAGE_BYTES) return fail(QCB_ERR_INVALID, "time slice exceeds staging buffer");
-  const int nt = slab_t(g);
+  const uint32_t V = L->dev.g.V;
   int k = 0;
-  for (int t0 = 0; t0 < g.L[3]; t0 += nt, k ^= 1) {
-    const int n = (t0 + nt <= g.L[3]) ? nt : g.L[3] - t0;
-    CU(launch_soa_to_aos(L->dev, c->d_stage[k], t0, n, bswap, c->stream, 0), "SoA->AoS");
+  for (uint32_t s0 = 0; s0 < V; s0 += STAGE_SITES, k ^= 1) {
+    const uint32_t n = (V - s0 < STAGE_SITES) ? V - s0 : STAGE_SITES;
+    CU(launch_soa_to_aos(L->dev, c->d_stage[k], s0, n, bswap, c->stream, 0), "SoA->AoS");
     c->launches++;
-    CU(cudaMemcpyAsync(host + (size_t)t0 * per_t, c->d_stage[k], (size_t)n * per_t * sizeof(double),
+    CU(cudaMemcpyAsync(host + (size_t)s0 * 72, c->d_stage[k], (size_t)n * 72 * sizeof(double),
                        cudaMemcpyDeviceToHost, c->stream),
        "D2H copy");
   }
@@ -495,20 +493,15 @@ int qcb_save_ildg(qcb_lattice* L, const char* path) {
     return fail(QCB_ERR_IO, std::string("write failed: ") + path);
   }
   int r = ensure_stage(c);
-  if (r == QCB_OK && !c->h_stage && cudaMallocHost(&c->h_stage, STAGE_BYTES) != cudaSuccess) {
-    cudaGetLastError();
-    r = fail(QCB_ERR_NOMEM, "cannot allocate pinned staging buffer");
-  }
+  if (r == QCB_OK) r = ensure_host_stage(c);
   if (r != QCB_OK) {
     fclose(fp);
     return r;
   }
-  const size_t per_t = (size_t)g.str[3] * 72;
-  const int nt = slab_t(g);
-  for (int t0 = 0; t0 < g.L[3]; t0 += nt) {
-    const int n = (t0 + nt <= g.L[3]) ? nt : g.L[3] - t0;
-    const size_t bytes = (size_t)n * per_t * sizeof(double);
-    cudaError_t e = launch_soa_to_aos(L->dev, c->d_stage[0], t0, n, 1, c->stream, 0);
+  for (uint32_t s0 = 0; s0 < g.V; s0 += STAGE_SITES) {
+    const uint32_t n = (g.V - s0 < STAGE_SITES) ? g.V - s0 : STAGE_SITES;
+    const size_t bytes = (size_t)n * 72 * sizeof(double);
+    cudaError_t e = launch_soa_to_aos(L->dev, c->d_stage[0], s0, n, 1, c->stream, 0);
     c->launches++;
     if (e == cudaSuccess) e = cudaMemcpyAsync(c->h_stage, c->d_stage[0], bytes, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -548,20 +541,15 @@ int qcb_load_ildg(qcb_lattice* L, const char* path) {
                                     " does not match the lattice (" + std::to_string(expected) + " bytes)");
   }
   r = ensure_stage(c);
-  if (r == QCB_OK && !c->h_stage && cudaMallocHost(&c->h_stage, STAGE_BYTES) != cudaSuccess) {
-    cudaGetLastError();
-    r = fail(QCB_ERR_NOMEM, "cannot allocate pinned staging buffer");
-  }
+  if (r == QCB_OK) r = ensure_host_stage(c);
   if (r != QCB_OK || fseeko(fp, (off_t)off, SEEK_SET) != 0) {
     fclose(fp);
     return r != QCB_OK ? r : fail(QCB_ERR_IO, "seek failed");
   }
-  const size_t per_t = (size_t)g.str[3] * 72;
-  const int nt = slab_t(g);
-  for (int t0 = 0; t0 < g.L[3]; t0 += nt) {
-    const int n = (t0 + nt <= g.L[3]) ? nt : g.L[3] - t0;
-    const size_t bytes = (size_t)n * per_t * sizeof(double);
-    cudaError_t e = cudaStreamSynchronize(c->stream);  // h_stage reuse
+  for (uint32_t s0 = 0; s0 < g.V; s0 += STAGE_SITES) {
+    const uint32_t n = (g.V - s0 < STAGE_SITES) ? g.V - s0 : STAGE_SITES;
+    const size_t bytes = (size_t)n * 72 * sizeof(double);
+    cudaError_t e = cudaStreamSynchronize(c->stream);  // h_stage is reused
     if (e != cudaSuccess) {
       fclose(fp);
       return cuda_fail(e, "ILDG upload");
@@ -571,7 +559,7 @@ int qcb_load_ildg(qcb_lattice* L, const char* path) {
       return fail(QCB_ERR_FORMAT, std::string(path) + ": truncated binary data");
     }
     e = cudaMemcpyAsync(c->d_stage[0], c->h_stage, bytes, cudaMemcpyHostToDevice, c->stream);
-    if (e == cudaSuccess) e = launch_aos_to_soa(L->dev, c->d_stage[0], t0, n, 1, c->stream, 0);
+    if (e == cudaSuccess) e = launch_aos_to_soa(L->dev, c->d_stage[0], s0, n, 1, c->stream, 0);
     c->launches++;
     if (e != cudaSuccess) {
       fclose(fp);

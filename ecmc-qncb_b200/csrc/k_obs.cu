@@ -173,6 +173,17 @@ __device__ __forceinline__ R sqnorm(const m3<R>& a) {
   return s;
 }
 
+// q and e contributions of one pair of planes, sgn * Re tr(F_{M1 N1} F_{M2 N2}) and the two
+// squared norms.  Not inlined: each pair is a separate register allocation, which keeps
+// the six clover evaluations of a site from being interleaved into one block that spills.
+template <typename S, int NR, typename R, int M1, int N1, int M2, int N2>
+__device__ __noinline__ void pair_qe(Geom g, Links<S, NR> f, Coord x, int par, uint32_t i, R sgn, R* q, R* e) {
+  const m3<R> Fa = clover_F<S, NR, R, M1, N1>(g, f, x, par, i);
+  const m3<R> Fb = clover_F<S, NR, R, M2, N2>(g, f, x, par, i);
+  *q += sgn * re_tr_nn(Fa, Fb);
+  *e += sqnorm(Fa) + sqnorm(Fb);
+}
+
 template <typename S, int NR>
 __global__ void __launch_bounds__(RED_THREADS) k_clover_qe(Geom g, Links<S, NR> f, double* __restrict__ parts) {
   typedef S R;
@@ -184,24 +195,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_clover_qe(Geom g, Links<S, NR> 
     const uint32_t i = (uint32_t)(t - (par ? g.Vh : 0));
     const Coord x = cb_coord(g, par, i);
     R q = 0, e = 0;
-    {
-      m3<R> Fa = clover_F<S, NR, R, 0, 1>(g, f, x, par, i);
-      m3<R> Fb = clover_F<S, NR, R, 2, 3>(g, f, x, par, i);
-      q += re_tr_nn(Fa, Fb);
-      e += sqnorm(Fa) + sqnorm(Fb);
-    }
-    {
-      m3<R> Fa = clover_F<S, NR, R, 0, 2>(g, f, x, par, i);
-      m3<R> Fb = clover_F<S, NR, R, 1, 3>(g, f, x, par, i);
-      q -= re_tr_nn(Fa, Fb);
-      e += sqnorm(Fa) + sqnorm(Fb);
-    }
-    {
-      m3<R> Fa = clover_F<S, NR, R, 0, 3>(g, f, x, par, i);
-      m3<R> Fb = clover_F<S, NR, R, 1, 2>(g, f, x, par, i);
-      q += re_tr_nn(Fa, Fb);
-      e += sqnorm(Fa) + sqnorm(Fb);
-    }
+    pair_qe<S, NR, R, 0, 1, 2, 3>(g, f, x, par, i, R(1), &q, &e);
+    pair_qe<S, NR, R, 0, 2, 1, 3>(g, f, x, par, i, R(-1), &q, &e);
+    pair_qe<S, NR, R, 0, 3, 1, 2>(g, f, x, par, i, R(1), &q, &e);
     accq += (double)q;
     acce += (double)e;
   }

@@ -174,15 +174,15 @@ __device__ __forceinline__ double bswap_d(double v) {
   return __longlong_as_double(((unsigned long long)lo << 32) | hi);
 }
 
-// One thread per (site of the slab, mu).  aos points at the slab's first site.
+// One thread per (site of the chunk, mu).  aos points at the chunk's first site, site0.
 template <typename S, int NR>
-__global__ void k_aos_to_soa(Geom g, Links<S, NR> f, const double* __restrict__ aos, int t0, uint32_t nsites,
-                             int bswap) {
+__global__ void k_aos_to_soa(Geom g, Links<S, NR> f, const double* __restrict__ aos, uint32_t site0,
+                             uint32_t nsites, int bswap) {
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (uint64_t)nsites * 4) return;
   const uint32_t sl = (uint32_t)(t >> 2);
   const int mu = (int)(t & 3);
-  const uint32_t s = (uint32_t)t0 * (uint32_t)g.str[3] + sl;
+  const uint32_t s = site0 + sl;
   // parity of s
   uint32_t r = s;
   const int x = (int)(r % (uint32_t)g.L[0]);
@@ -207,12 +207,13 @@ __global__ void k_aos_to_soa(Geom g, Links<S, NR> f, const double* __restrict__ 
 }
 
 template <typename S, int NR>
-__global__ void k_soa_to_aos(Geom g, Links<S, NR> f, double* __restrict__ aos, int t0, uint32_t nsites, int bswap) {
+__global__ void k_soa_to_aos(Geom g, Links<S, NR> f, double* __restrict__ aos, uint32_t site0, uint32_t nsites,
+                             int bswap) {
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (uint64_t)nsites * 4) return;
   const uint32_t sl = (uint32_t)(t >> 2);
   const int mu = (int)(t & 3);
-  const uint32_t s = (uint32_t)t0 * (uint32_t)g.str[3] + sl;
+  const uint32_t s = site0 + sl;
   uint32_t r = s;
   const int x = (int)(r % (uint32_t)g.L[0]);
   r /= (uint32_t)g.L[0];
@@ -236,29 +237,30 @@ __global__ void k_soa_to_aos(Geom g, Links<S, NR> f, double* __restrict__ aos, i
 }
 
 template <typename S, int NR>
-static cudaError_t a2s_impl(const LatDev& L, const double* aos, int t0, int nt, int bswap, cudaStream_t s,
-                            int block) {
-  const uint32_t nsites = (uint32_t)nt * (uint32_t)L.g.str[3];
-  k_aos_to_soa<S, NR><<<grid_for((uint64_t)nsites * 4, block), block, 0, s>>>(L.g, links_of<S, NR>(L), aos, t0,
+static cudaError_t a2s_impl(const LatDev& L, const double* aos, uint32_t site0, uint32_t nsites, int bswap,
+                            cudaStream_t s, int block) {
+  k_aos_to_soa<S, NR><<<grid_for((uint64_t)nsites * 4, block), block, 0, s>>>(L.g, links_of<S, NR>(L), aos, site0,
                                                                                nsites, bswap);
   return cudaGetLastError();
 }
 template <typename S, int NR>
-static cudaError_t s2a_impl(const LatDev& L, double* aos, int t0, int nt, int bswap, cudaStream_t s, int block) {
-  const uint32_t nsites = (uint32_t)nt * (uint32_t)L.g.str[3];
-  k_soa_to_aos<S, NR><<<grid_for((uint64_t)nsites * 4, block), block, 0, s>>>(L.g, links_of<S, NR>(L), aos, t0,
+static cudaError_t s2a_impl(const LatDev& L, double* aos, uint32_t site0, uint32_t nsites, int bswap,
+                            cudaStream_t s, int block) {
+  k_soa_to_aos<S, NR><<<grid_for((uint64_t)nsites * 4, block), block, 0, s>>>(L.g, links_of<S, NR>(L), aos, site0,
                                                                                nsites, bswap);
   return cudaGetLastError();
 }
-cudaError_t launch_aos_to_soa(const LatDev& L, const double* aos, int t0, int nt, int bswap, cudaStream_t s,
-                              int block) {
+cudaError_t launch_aos_to_soa(const LatDev& L, const double* aos, uint32_t site0, uint32_t nsites, int bswap,
+                              cudaStream_t s, int block) {
   if (block <= 0) block = 256;
-  QCB_DISPATCH_STORE(L, a2s_impl, L, aos, t0, nt, bswap, s, block);
+  if ((uint64_t)site0 + nsites > L.g.V) return cudaErrorInvalidValue;
+  QCB_DISPATCH_STORE(L, a2s_impl, L, aos, site0, nsites, bswap, s, block);
 }
-cudaError_t launch_soa_to_aos(const LatDev& L, double* aos, int t0, int nt, int bswap, cudaStream_t s,
-                              int block) {
+cudaError_t launch_soa_to_aos(const LatDev& L, double* aos, uint32_t site0, uint32_t nsites, int bswap,
+                              cudaStream_t s, int block) {
   if (block <= 0) block = 256;
-  QCB_DISPATCH_STORE(L, s2a_impl, L, aos, t0, nt, bswap, s, block);
+  if ((uint64_t)site0 + nsites > L.g.V) return cudaErrorInvalidValue;
+  QCB_DISPATCH_STORE(L, s2a_impl, L, aos, site0, nsites, bswap, s, block);
 }
 
 // ---- precision / storage conversion ---------------------------------------------------

@@ -29,11 +29,11 @@ cudaError_t launch_cold(const LatDev& L, cudaStream_t s, int block);
 cudaError_t launch_hot(const LatDev& L, uint64_t seed, cudaStream_t s, int block);
 cudaError_t launch_gauge_transform(const LatDev& L, uint64_t seed, cudaStream_t s, int block);
 cudaError_t launch_reunitarize(const LatDev& L, cudaStream_t s, int block);
-// AoS FP64 (72 doubles per site, ILDG order) for the t-slab [t0, t0+nt) <-> lattice.
-cudaError_t launch_aos_to_soa(const LatDev& L, const double* aos, int t0, int nt, int bswap, cudaStream_t s,
-                              int block);
-cudaError_t launch_soa_to_aos(const LatDev& L, double* aos, int t0, int nt, int bswap, cudaStream_t s,
-                              int block);
+// AoS FP64 (72 doubles per site, ILDG order) for the sites [site0, site0+nsites) <-> lattice.
+cudaError_t launch_aos_to_soa(const LatDev& L, const double* aos, uint32_t site0, uint32_t nsites, int bswap,
+                              cudaStream_t s, int block);
+cudaError_t launch_soa_to_aos(const LatDev& L, double* aos, uint32_t site0, uint32_t nsites, int bswap,
+                              cudaStream_t s, int block);
 cudaError_t launch_convert(const LatDev& dst, const LatDev& src, cudaStream_t s, int block);
 
 // ---- heatbath (k_hb.cu) ------------------------------------------------------------
