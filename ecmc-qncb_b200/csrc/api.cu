@@ -28,6 +28,8 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 }  // namespace
 
+int qcb::set_error(int code, const char* msg) { return fail(code, msg); }
+
 #define CU(call, what)                               \
   do {                                               \
     cudaError_t e_ = (call);                         \

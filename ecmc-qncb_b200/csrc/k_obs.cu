@@ -110,6 +110,25 @@ cudaError_t launch_plaquette(const LatDev& L, double* scratch, double* out, cuda
   QCB_DISPATCH_STORE(L, plaquette_impl, L, scratch, out, s, block);
 }
 
+// Same reduction with a caller-chosen number of blocks (partials written to scratch[0..nblocks)).
+template <typename S, int NR>
+static cudaError_t plaquette_partials_impl(const LatDev& L, int nblocks, double* scratch, double* out,
+                                           cudaStream_t s) {
+  Links<S, NR> f;
+  f.p = reinterpret_cast<typename Links<S, NR>::V*>(L.links);
+  f.stride = L.g.stride;
+  k_plaquette<S, NR><<<nblocks, RED_THREADS, 0, s>>>(L.g, f, scratch);
+  k_finalize<<<1, 32, 0, s>>>(scratch, nblocks, 1, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_plaquette_partials(const LatDev& L, int nblocks, double* scratch, double* out, cudaStream_t s) {
+  if (nblocks < 1) return cudaErrorInvalidValue;
+  QCB_DISPATCH_STORE(L, plaquette_partials_impl, L, nblocks, scratch, out, s);
+}
+
+int reduce_threads() { return RED_THREADS; }
+
 // ---- clover Q and E -------------------------------------------------------------------
 // Clover sum C_{mu nu}(x) of the four leaves, in the reference's leaf order
 // (observables_mpi.cpp:70-80).

@@ -49,11 +49,17 @@ cudaError_t launch_hb_pass(const LatDev& L, int mu, int parity, double beta, uin
 int reduce_blocks();
 cudaError_t launch_plaquette(const LatDev& L, double* scratch, double* out, cudaStream_t s, int block);
 cudaError_t launch_clover_qe(const LatDev& L, double* scratch, double* out2, cudaStream_t s, int block);
+// Plaquette sum with nblocks reduction blocks (scratch holds nblocks doubles); out[0] = sum.
+cudaError_t launch_plaquette_partials(const LatDev& L, int nblocks, double* scratch, double* out, cudaStream_t s);
+int reduce_threads();
 
 // ---- flow (k_flow.cu) --------------------------------------------------------------
 // RK3 stage k (1, 2, 3) of Luescher's integrator: reads links from src, the force
 // accumulator z, writes links to dst.
 cudaError_t launch_flow_stage(int stage, const LatDev& src, const LatDev& dst, const AlgDev& z, double eps,
                               cudaStream_t s, int block);
+
+// Sets the calling thread's qcb_last_error() message; returns code.
+int set_error(int code, const char* msg);
 
 }  // namespace qcb

@@ -76,6 +76,7 @@ SIGNATURES = {
     "qcb_topo_qe": (C.c_int, [_vp, _dp, _dp]),
     "qcb_flow_measure": (C.c_int, [_vp, C.c_double, C.c_int, C.c_int, _dp]),
     "qcb_flow_steps": (C.c_int, [_vp, C.c_double, C.c_int]),
+    "qcb_plaquette_noalloc": (C.c_int, [_vp, _ip, C.c_int, C.c_int, C.c_size_t, _vp, _vp]),
     "qcb_params_default": (C.c_int, [C.POINTER(HbParams)]),
     "qcb_params_load": (C.c_int, [C.c_char_p, C.POINTER(HbParams)]),
 }

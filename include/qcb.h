@@ -134,6 +134,22 @@ int qcb_plaquette(qcb_lattice* lat, double* out);
  * density E = (1/V) sum_x 1/2 sum_{mu<nu} |F_{mu nu}|^2 with F = (C - C^dagger)/8. */
 int qcb_topo_qe(qcb_lattice* lat, double* q, double* e);
 
+/* ---- allocation-free plaquette ---------------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device memory (a
+ * host whose pool allocator owns the device memory, or a loop where cudaMalloc's implicit
+ * device synchronisation is not acceptable): the mean plaquette of links already on the
+ * device, in this library's layout (dims, precision, storage and stride as reported by
+ * qcb_lattice_device_links), written to out[0] (caller-owned device memory) on `stream`
+ * (a cudaStream_t; NULL = legacy default stream), asynchronously.  It calls no cudaMalloc,
+ * cudaFree or other allocating routine: its reduction scratch is a static device array of
+ * QCB_NOALLOC_MAX_PARTIALS doubles (16 KiB per GPU, held until the process exits).  The
+ * first call on a device looks up that array's device address (make it before any stream
+ * capture).  Calls share the array, so calls that overlap on the GPU race; requests that
+ * would need more partial sums than the array holds are rejected with QCB_ERR_INVALID. */
+#define QCB_NOALLOC_MAX_PARTIALS 2048
+int qcb_plaquette_noalloc(const void* links, const int dims[4], int precision, int storage, size_t stride,
+                          double* out, void* stream);
+
 /* ---- Wilson flow -------------------------------------------------------------------
  * mpi::observables::topo_charge_flowed (observables_mpi.cpp:153-178) with
  * GradientFlow::rk3_step (src/flow/gradient_flow.cpp:15-128): on a copy of the links,
