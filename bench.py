@@ -282,6 +282,28 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     return result
 
 
+def profile_steps(args) -> int:
+    """warmup + steps of the workload only, nothing else; prints the kernel launch counts so
+    that an ncu capture can skip the warm-up launches (-s) and take one step (-c)."""
+    import qcb
+    from qcb import _lib
+
+    ctx = qcb.Context(0)
+    prec, nr = ("fp32", 12) if args.storage == "fp32-12" else ("fp64", 18)
+    f = qcb.GaugeField(ctx, (L, L, L, L), prec, nr)
+    gf = qcb.GradientFlow(FLOW_EPS)
+    counts = []
+    for _ in range(args.warmup + args.steps):
+        n0 = ctx.launches()
+        f.hot_start(SEED)
+        _lib.check(_lib.lib().qcb_heatbath(f.h, BETA, SWEEPS, 1, SEED, 0))
+        qcb.observables.topo_charge_flowed(f, gf, FLOW_RECORDS, FLOW_RK)
+        ctx.sync()
+        counts.append(ctx.launches() - n0)
+    print(json.dumps({"profile": args.storage, "launches_per_step": counts}))
+    return 0
+
+
 # ---------------------------------------------------------------------------------------
 def _ref_worker(args):
     """One 'rank' of the reference schedule on a block of edge lb: sweeps then flow."""
@@ -328,6 +350,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="run only warmup + steps of the workload (for ncu); print launch counts")
+    ap.add_argument("--storage", choices=["fp32-12", "fp64-18"], default="fp32-12")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -368,6 +393,8 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                  device_id=torch.device("cuda", local_rank))
         dist = tdist
+    if args.profile:
+        return profile_steps(args)
     try:
         res = run_ours(args, rank, world, local_rank, dist)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:

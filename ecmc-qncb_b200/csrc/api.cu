@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/qcb.h"
+#include "api_internal.h"
 #include "host_io.h"
 #include "kernels.h"
 
@@ -36,32 +37,6 @@ int qcb::set_error(int code, const char* msg) { return fail(code, msg); }
     if (e_ != cudaSuccess) return cuda_fail(e_, what); \
   } while (0)
 
-// ---- objects -------------------------------------------------------------------------------
-struct qcb_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int block = 0;
-  uint32_t* d_status = nullptr;  // [0] KP cap hits
-  uint32_t* h_status = nullptr;  // pinned mirror
-  double* d_scratch = nullptr;   // reduction partials
-  double* d_out = nullptr;       // small results
-  double* h_out = nullptr;       // pinned mirror
-  double* d_stage[2] = {nullptr, nullptr};
-  size_t stage_bytes = 0;
-  double* h_stage = nullptr;  // pinned, for file I/O
-  uint64_t launches = 0;
-  std::mutex mu;
-};
-
-struct qcb_lattice {
-  qcb_ctx* ctx = nullptr;
-  LatDev dev;
-  size_t bytes = 0;
-  // Wilson-flow work space, allocated on first use: two link buffers + accumulator.
-  void* fw[2] = {nullptr, nullptr};
-  void* fz = nullptr;
-};
-
 namespace {
 constexpr size_t STAGE_BYTES = 64ull << 20;
 
@@ -70,8 +45,10 @@ int set_device(qcb_ctx* c) {
   return QCB_OK;
 }
 
+}  // namespace
+
 // Reads and clears the device status words; reports KP cap hits.
-int check_status(qcb_ctx* c) {
+int qcb::check_status(qcb_ctx* c) {
   CU(cudaMemcpyAsync(c->h_status, c->d_status, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream),
      "status copy");
   CU(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
@@ -85,6 +62,7 @@ int check_status(qcb_ctx* c) {
   return QCB_OK;
 }
 
+namespace {
 int valid_dims(const int dims[4]) {
   if (!dims) return 0;
   uint64_t v = 1;
@@ -95,7 +73,9 @@ int valid_dims(const int dims[4]) {
   return v < (1ull << 30);  // link ids mu*V + s must fit in 32 bits
 }
 
-int ensure_flow_space(qcb_lattice* L) {
+}  // namespace
+
+int qcb::ensure_flow_space(qcb_lattice* L) {
   if (L->fw[0]) return QCB_OK;
   const size_t lb = link_bytes(L->dev.g, L->dev.prec, L->dev.nr);
   const size_t ab = alg_bytes(L->dev.g, L->dev.prec);
@@ -111,6 +91,7 @@ int ensure_flow_space(qcb_lattice* L) {
   return QCB_OK;
 }
 
+namespace {
 LatDev with_links(const LatDev& d, void* p) {
   LatDev r = d;
   r.links = p;

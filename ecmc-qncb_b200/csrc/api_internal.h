@@ -1,0 +1,39 @@
+// api_internal.h — the C ABI's opaque objects and shared host helpers (library-internal).
+#pragma once
+#include <mutex>
+#include <string>
+
+#include "../../include/qcb.h"
+#include "kernels.h"
+
+struct qcb_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int block = 0;
+  uint32_t* d_status = nullptr;  // [0] KP cap hits
+  uint32_t* h_status = nullptr;  // pinned mirror
+  double* d_scratch = nullptr;   // reduction partials
+  double* d_out = nullptr;       // small results
+  double* h_out = nullptr;       // pinned mirror
+  double* d_stage[2] = {nullptr, nullptr};
+  size_t stage_bytes = 0;
+  double* h_stage = nullptr;  // pinned, for file I/O
+  uint64_t launches = 0;
+  std::mutex mu;
+};
+
+struct qcb_lattice {
+  qcb_ctx* ctx = nullptr;
+  qcb::LatDev dev;
+  size_t bytes = 0;
+  // Wilson-flow work space, allocated on first use: two link buffers + accumulator.
+  void* fw[2] = {nullptr, nullptr};
+  void* fz = nullptr;
+};
+
+namespace qcb {
+// Allocates a lattice's Wilson-flow work space (two link buffers + accumulator) once.
+int ensure_flow_space(qcb_lattice* L);
+// Reads and clears the context's device status words (after synchronising its stream).
+int check_status(qcb_ctx* c);
+}  // namespace qcb

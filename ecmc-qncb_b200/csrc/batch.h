@@ -1,0 +1,52 @@
+// batch.h — device descriptors and launchers of the persistent multi-lattice kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kernels.h"
+
+namespace qcb {
+
+// One lattice of a batched launch (device array).
+struct BatchLat {
+  Geom g;
+  void* links;      // heatbath: the links; flow: buffer a of even steps
+  void* work;       // flow: buffer b of even steps
+  void* acc;        // flow: force accumulator
+  double beta;      // heatbath coupling
+  uint32_t k0, k1;  // Philox key (seed)
+  uint32_t sweep0;  // sweep counter of the launch's first sweep
+  uint32_t tile;    // sites per work item (any multiple of the block size)
+  uint32_t ntiles;  // work items of this lattice per level (flow: 8 x site tiles)
+};
+
+// One persistent launch: nlevels levels of per_level items each.
+struct BatchRun {
+  const BatchLat* lats;    // nlat descriptors
+  const uint32_t* prefix;  // nlat+1 prefix sums of ntiles; prefix[nlat] = per_level
+  int nlat;
+  uint32_t nlevels;
+  uint32_t per_level;
+  uint32_t* done;    // nlat finished-tile counters, zero at launch
+  uint32_t* status;  // [0] KP cap hits, [1] wait timeouts, [2] abort flag
+  int n_hits;
+  double eps;
+};
+
+enum : int { BATCH_HB = 0, BATCH_FLOW = 1 };
+
+// Cooperative persistent launch: the grid is the co-resident maximum (capped by
+// max_blocks when > 0) for the given block size.
+cudaError_t launch_batch(int kind, const BatchRun& run, int prec, int nr, int block, int max_blocks,
+                         cudaStream_t s);
+
+// Batched reductions: one item per (lattice, tile of RED sites), item r of lattice l in
+// [rprefix[l], rprefix[l+1]).  out[l] = mean plaquette; out2[2l], out2[2l+1] = (Q, E).
+// scratch holds 2 * rprefix[nlat] doubles.
+int batch_red_sites();
+cudaError_t launch_batch_plaquette(const BatchLat* lats, const uint32_t* rprefix, int nlat, uint32_t nitems,
+                                   int prec, int nr, double* scratch, double* out, cudaStream_t s);
+cudaError_t launch_batch_qe(const BatchLat* lats, const uint32_t* rprefix, int nlat, uint32_t nitems, int prec,
+                            int nr, double* scratch, double* out2, cudaStream_t s);
+
+}  // namespace qcb

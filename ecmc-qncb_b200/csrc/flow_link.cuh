@@ -1,0 +1,88 @@
+// flow_link.cuh — one link of one fused Wilson-flow RK3 stage (shared by the
+// single-lattice stage kernel and the persistent batched kernel).
+//
+// Reference: GradientFlow (src/flow/gradient_flow.cpp:15-114):
+//   Z   = -P_TA(U A)                         (force, gradient_flow.cpp:15-34)
+//   s1: X = eps/4 Z0;                acc = Z0                      (compute_w1, :37-53)
+//   s2: X = 8/9 eps Z1 - 17/36 eps Z0; acc = 8/9 Z1 - 17/36 Z0    (compute_w2 + replace_force_0, :56-93)
+//   s3: X = 3/4 eps Z2 - eps acc                                   (compute_w3, :96-114)
+//   U' = exp(X) U   with Luescher's exponential (src/su3/utils.cpp:145-193)
+#pragma once
+#include "staple.cuh"
+
+namespace qcb {
+
+template <typename F, typename ACC, typename R, int STAGE, int MU>
+__device__ __forceinline__ void flow_link(const Geom& g, const F& src, const F& dst, const ACC& acc, R eps, int par,
+                                          uint32_t i) {
+  const Coord x = cb_coord(g, par, i);
+  const m3<R> A = staple_sum<F, R, MU>(g, src, x, par, i);
+  const m3<R> U = src.template load<R>(MU, par, i);
+  // Z = P_TA(-U A) = -P_TA(U A)
+  alg8<R> Z = proj_ta(mul_nn(U, A));
+#pragma unroll
+  for (int k = 0; k < 8; ++k) Z.a[k] = -Z.a[k];
+  alg8<R> X;
+  if (STAGE == 1) {
+    const R c = R(0.25) * eps;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) X.a[k] = c * Z.a[k];
+    acc.template store<R>(MU, par, i, Z);
+  } else if (STAGE == 2) {
+    const alg8<R> Z0 = acc.template load<R>(MU, par, i);
+    const R c1 = R(8.0 / 9.0) * eps, c0 = R(17.0 / 36.0) * eps;
+    alg8<R> N;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      X.a[k] = c1 * Z.a[k] - c0 * Z0.a[k];
+      N.a[k] = R(8.0 / 9.0) * Z.a[k] - R(17.0 / 36.0) * Z0.a[k];
+    }
+    acc.template store<R>(MU, par, i, N);
+  } else {
+    const alg8<R> Z0 = acc.template load<R>(MU, par, i);
+    const R c1 = R(0.75) * eps;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) X.a[k] = c1 * Z.a[k] - eps * Z0.a[k];
+  }
+  const m3<R> E = exp_su3(X);
+  dst.template store<R>(MU, par, i, mul_nn(E, U));
+}
+
+// Runtime-direction variant (one code path for every mu).
+template <typename F, typename ACC, typename R, int STAGE>
+__device__ __forceinline__ void flow_link_rt(const Geom& g, const F& src, const F& dst, const ACC& acc, R eps, int MU,
+                                             int par, uint32_t i) {
+  const Coord x = cb_coord(g, par, i);
+  const m3<R> A = staple_sum_rt<F, R>(g, src, x, MU, par, i);
+  const m3<R> U = src.template load<R>(MU, par, i);
+  // Z = P_TA(-U A) = -P_TA(U A)
+  alg8<R> Z = proj_ta(mul_nn(U, A));
+#pragma unroll
+  for (int k = 0; k < 8; ++k) Z.a[k] = -Z.a[k];
+  alg8<R> X;
+  if (STAGE == 1) {
+    const R c = R(0.25) * eps;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) X.a[k] = c * Z.a[k];
+    acc.template store<R>(MU, par, i, Z);
+  } else if (STAGE == 2) {
+    const alg8<R> Z0 = acc.template load<R>(MU, par, i);
+    const R c1 = R(8.0 / 9.0) * eps, c0 = R(17.0 / 36.0) * eps;
+    alg8<R> N;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      X.a[k] = c1 * Z.a[k] - c0 * Z0.a[k];
+      N.a[k] = R(8.0 / 9.0) * Z.a[k] - R(17.0 / 36.0) * Z0.a[k];
+    }
+    acc.template store<R>(MU, par, i, N);
+  } else {
+    const alg8<R> Z0 = acc.template load<R>(MU, par, i);
+    const R c1 = R(0.75) * eps;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) X.a[k] = c1 * Z.a[k] - eps * Z0.a[k];
+  }
+  const m3<R> E = exp_su3(X);
+  dst.template store<R>(MU, par, i, mul_nn(E, U));
+}
+
+}  // namespace qcb

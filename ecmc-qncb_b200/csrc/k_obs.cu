@@ -11,6 +11,7 @@
 // summed in a fixed order with Neumaier compensation by a single-block kernel.  The grid
 // is a fixed multiple of the SM count (grid-stride loop), so the scratch is bounded.
 #include "dispatch.cuh"
+#include "obs_site.cuh"
 
 namespace qcb {
 
@@ -41,44 +42,41 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return r;
 }
 
-// Neumaier-compensated sum of n partials (one block), written to out[0].
-__global__ void k_finalize(const double* __restrict__ parts, int n, int nq, double* __restrict__ out) {
-  // thread q sums quantity q sequentially (n is ~1k): fixed order, compensated.
-  const int q = threadIdx.x;
-  if (q >= nq) return;
-  double s = 0.0, c = 0.0;
-  for (int k = 0; k < n; ++k) {
-    double v = parts[q * n + k];
-    double t = s + v;
-    if (fabs(s) >= fabs(v))
-      c += (s - t) + v;
-    else
-      c += (v - t) + s;
-    s = t;
-  }
-  out[q] = s + c;
+__device__ __forceinline__ void neumaier_add(double& s, double& c, double v) {
+  const double t = s + v;
+  if (fabs(s) >= fabs(v))
+    c += (s - t) + v;
+  else
+    c += (v - t) + s;
+  s = t;
 }
 
-// ---- plaquette ------------------------------------------------------------------------
-template <typename S, int NR, typename R>
-__device__ __forceinline__ R site_plaquette(const Geom& g, const Links<S, NR>& f, const Coord& x, int par,
-                                            uint32_t i) {
-  const int opp = par ^ 1;
-  R sum = 0;
-#pragma unroll
-  for (int mu = 0; mu < 4; ++mu) {
-    const m3<R> Umu = f.template load<R>(mu, par, i);
-    const uint32_t xmu = cb_index(nb_full(g, x, mu, +1));
-#pragma unroll
-    for (int nu = mu + 1; nu < 4; ++nu) {
-      const uint32_t xnu = cb_index(nb_full(g, x, nu, +1));
-      // T1 = U_mu(x) U_nu(x+mu), T2 = U_nu(x) U_mu(x+nu); Re tr(T1 T2^dag)
-      m3<R> T1 = mul_nn(Umu, f.template load<R>(nu, opp, xmu));
-      m3<R> T2 = mul_nn(f.template load<R>(nu, par, i), f.template load<R>(mu, opp, xnu));
-      sum += re_tr_na(T1, T2);
+// Neumaier-compensated sums of nq quantities of n partials each (parts[q*n + k]), one warp
+// per quantity: lane j sums k = j, j+32, ...; lane 0 then adds the 32 lane sums in lane
+// order.  The order is fixed, so the result is deterministic.  out[q] = sum.
+__global__ void k_finalize(const double* __restrict__ parts, int n, int nq, double* __restrict__ out) {
+  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (q >= nq) return;
+  double s = 0.0, c = 0.0;
+  for (int k = lane; k < n; k += 32) neumaier_add(s, c, parts[q * n + k]);
+  __shared__ double ls[4][32], lc[4][32];
+  ls[q][lane] = s;
+  lc[q][lane] = c;
+  __syncwarp();
+  if (lane == 0) {
+    double S = 0.0, Cc = 0.0;
+    for (int j = 0; j < 32; ++j) {
+      neumaier_add(S, Cc, ls[q][j]);
+      Cc += lc[q][j];
     }
+    out[q] = S + Cc;
   }
-  return sum * R(1.0 / 3.0);
+}
+
+// Reduction grid: one block per RED_THREADS sites, at most RED_BLOCKS.
+static int red_grid(const Geom& g) {
+  const uint64_t want = ((uint64_t)g.V + RED_THREADS - 1) / RED_THREADS;
+  return (int)(want < (uint64_t)RED_BLOCKS ? want : (uint64_t)RED_BLOCKS);
 }
 
 template <typename S, int NR>
@@ -90,7 +88,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_plaquette(Geom g, Links<S, NR> 
     const int par = (t >= g.Vh) ? 1 : 0;
     const uint32_t i = (uint32_t)(t - (par ? g.Vh : 0));
     const Coord x = cb_coord(g, par, i);
-    acc += (double)site_plaquette<S, NR, S>(g, f, x, par, i);
+    acc += (double)site_plaquette<Links<S, NR>, S>(g, f, x, par, i);
   }
   double b = block_sum<RED_THREADS>(acc, sh);
   if (threadIdx.x == 0) parts[blockIdx.x] = b;
@@ -101,8 +99,9 @@ static cudaError_t plaquette_impl(const LatDev& L, double* scratch, double* out,
   Links<S, NR> f;
   f.p = reinterpret_cast<typename Links<S, NR>::V*>(L.links);
   f.stride = L.g.stride;
-  k_plaquette<S, NR><<<RED_BLOCKS, RED_THREADS, 0, s>>>(L.g, f, scratch);
-  k_finalize<<<1, 32, 0, s>>>(scratch, RED_BLOCKS, 1, out);
+  const int nb = red_grid(L.g);
+  k_plaquette<S, NR><<<nb, RED_THREADS, 0, s>>>(L.g, f, scratch);
+  k_finalize<<<1, 32, 0, s>>>(scratch, nb, 1, out);
   return cudaGetLastError();
 }
 
@@ -129,80 +128,6 @@ cudaError_t launch_plaquette_partials(const LatDev& L, int nblocks, double* scra
 
 int reduce_threads() { return RED_THREADS; }
 
-// ---- clover Q and E -------------------------------------------------------------------
-// Clover sum C_{mu nu}(x) of the four leaves, in the reference's leaf order
-// (observables_mpi.cpp:70-80).
-template <typename S, int NR, typename R, int MU, int NU>
-__device__ __forceinline__ m3<R> clover_F(const Geom& g, const Links<S, NR>& f, const Coord& x, int par,
-                                          uint32_t i) {
-  const int opp = par ^ 1;
-  const uint32_t xpmu = cb_index(nb_full(g, x, MU, +1));            // opp
-  const uint32_t xpnu = cb_index(nb_full(g, x, NU, +1));            // opp
-  const uint32_t xmmu = cb_index(nb_full(g, x, MU, -1));            // opp
-  const uint32_t xmnu = cb_index(nb_full(g, x, NU, -1));            // opp
-  const uint32_t xmmupnu = cb_index(nb2_full(g, x, MU, -1, NU, +1));  // par
-  const uint32_t xmmumnu = cb_index(nb2_full(g, x, MU, -1, NU, -1));  // par
-  const uint32_t xpmumnu = cb_index(nb2_full(g, x, MU, +1, NU, -1));  // par
-  const m3<R> Umu_x = f.template load<R>(MU, par, i);
-  const m3<R> Unu_x = f.template load<R>(NU, par, i);
-  m3<R> C;
-  {
-    // U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
-    m3<R> T1 = mul_nn(Umu_x, f.template load<R>(NU, opp, xpmu));
-    m3<R> T2 = mul_nn(Unu_x, f.template load<R>(MU, opp, xpnu));
-    C = mul_na(T1, T2);
-  }
-  const m3<R> Umu_xmmu = f.template load<R>(MU, opp, xmmu);
-  {
-    // U_nu(x) U_mu(x-mu+nu)^dag U_nu(x-mu)^dag U_mu(x-mu)
-    m3<R> T1 = mul_na(Unu_x, f.template load<R>(MU, par, xmmupnu));
-    m3<R> T2 = mul_an(f.template load<R>(NU, opp, xmmu), Umu_xmmu);
-    acc_nn(C, T1, T2);
-  }
-  const m3<R> Unu_xmnu = f.template load<R>(NU, opp, xmnu);
-  {
-    // U_mu(x-mu)^dag U_nu(x-mu-nu)^dag U_mu(x-mu-nu) U_nu(x-nu)
-    m3<R> T1 = mul_aa(Umu_xmmu, f.template load<R>(NU, par, xmmumnu));
-    m3<R> T2 = mul_nn(f.template load<R>(MU, par, xmmumnu), Unu_xmnu);
-    acc_nn(C, T1, T2);
-  }
-  {
-    // U_nu(x-nu)^dag U_mu(x-nu) U_nu(x+mu-nu) U_mu(x)^dag
-    m3<R> T1 = mul_an(Unu_xmnu, f.template load<R>(MU, opp, xmnu));
-    m3<R> T2 = mul_na(f.template load<R>(NU, par, xpmumnu), Umu_x);
-    acc_nn(C, T1, T2);
-  }
-  // F = (C - C^dag) / 8
-  m3<R> F;
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int b = 0; b < 3; ++b)
-      F.e[a][b] = mk<R>(R(0.125) * (C.e[a][b].re - C.e[b][a].re), R(0.125) * (C.e[a][b].im + C.e[b][a].im));
-  return F;
-}
-
-template <typename R>
-__device__ __forceinline__ R sqnorm(const m3<R>& a) {
-  R s = 0;
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) s = fma(a.e[i][j].re, a.e[i][j].re, fma(a.e[i][j].im, a.e[i][j].im, s));
-  return s;
-}
-
-// q and e contributions of one pair of planes, sgn * Re tr(F_{M1 N1} F_{M2 N2}) and the two
-// squared norms.  Not inlined: each pair is a separate register allocation, which keeps
-// the six clover evaluations of a site from being interleaved into one block that spills.
-template <typename S, int NR, typename R, int M1, int N1, int M2, int N2>
-__device__ __noinline__ void pair_qe(Geom g, Links<S, NR> f, Coord x, int par, uint32_t i, R sgn, R* q, R* e) {
-  const m3<R> Fa = clover_F<S, NR, R, M1, N1>(g, f, x, par, i);
-  const m3<R> Fb = clover_F<S, NR, R, M2, N2>(g, f, x, par, i);
-  *q += sgn * re_tr_nn(Fa, Fb);
-  *e += sqnorm(Fa) + sqnorm(Fb);
-}
-
 template <typename S, int NR>
 __global__ void __launch_bounds__(RED_THREADS) k_clover_qe(Geom g, Links<S, NR> f, double* __restrict__ parts) {
   typedef S R;
@@ -214,9 +139,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_clover_qe(Geom g, Links<S, NR> 
     const uint32_t i = (uint32_t)(t - (par ? g.Vh : 0));
     const Coord x = cb_coord(g, par, i);
     R q = 0, e = 0;
-    pair_qe<S, NR, R, 0, 1, 2, 3>(g, f, x, par, i, R(1), &q, &e);
-    pair_qe<S, NR, R, 0, 2, 1, 3>(g, f, x, par, i, R(-1), &q, &e);
-    pair_qe<S, NR, R, 0, 3, 1, 2>(g, f, x, par, i, R(1), &q, &e);
+    site_qe<Links<S, NR>, R>(g, f, x, par, i, &q, &e);
     accq += (double)q;
     acce += (double)e;
   }
@@ -224,7 +147,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_clover_qe(Geom g, Links<S, NR> 
   double be = block_sum<RED_THREADS>(acce, sh);
   if (threadIdx.x == 0) {
     parts[blockIdx.x] = bq;
-    parts[RED_BLOCKS + blockIdx.x] = be;
+    parts[gridDim.x + blockIdx.x] = be;
   }
 }
 
@@ -239,8 +162,9 @@ static cudaError_t clover_impl(const LatDev& L, double* scratch, double* out2, c
   Links<S, NR> f;
   f.p = reinterpret_cast<typename Links<S, NR>::V*>(L.links);
   f.stride = L.g.stride;
-  k_clover_qe<S, NR><<<RED_BLOCKS, RED_THREADS, 0, s>>>(L.g, f, scratch);
-  k_finalize<<<1, 32, 0, s>>>(scratch, RED_BLOCKS, 2, out2);
+  const int nb = red_grid(L.g);
+  k_clover_qe<S, NR><<<nb, RED_THREADS, 0, s>>>(L.g, f, scratch);
+  k_finalize<<<1, 64, 0, s>>>(scratch, nb, 2, out2);
   k_qe_scale<<<1, 1, 0, s>>>(out2, 1.0 / (double)L.g.V);
   return cudaGetLastError();
 }

@@ -106,7 +106,18 @@ struct Store<float, 12> {
   static constexpr int NC = 3;
 };
 
-template <typename S, int NR>
+// Load path of a link read.  LD_RO: read-only data path (__ldg), for kernels that never
+// read links written earlier in the same launch.  LD_CG: L2-coherent loads (__ldcg), for
+// persistent kernels whose blocks read links other blocks wrote in the same launch.
+enum : int { LD_RO = 0, LD_CG = 1 };
+
+template <int LM, typename V>
+__device__ __forceinline__ V ldv(const V* p) {
+  if (LM == LD_RO) return __ldg(p);
+  return __ldcg(p);
+}
+
+template <typename S, int NR, int LM = LD_RO>
 struct Links {
   typedef typename Store<S, NR>::V V;
   static constexpr int NC = Store<S, NR>::NC;
@@ -119,92 +130,52 @@ struct Links {
 
   // Load link (mu, par, i) as an m3<R> (row 2 rebuilt for 12-real storage).
   template <typename R>
-  __device__ __forceinline__ m3<R> load(int mu, int par, uint32_t i) const;
+  __device__ __forceinline__ m3<R> load(int mu, int par, uint32_t i) const {
+    m3<R> u;
+    if constexpr (sizeof(V) == 4 * sizeof(S)) {
+      // FP32 12-real: three float4 chunks (e00,e01), (e02,e10), (e11,e12).
+      const V a = ldv<LM>(&p[idx(mu, par, 0, i)]);
+      const V b = ldv<LM>(&p[idx(mu, par, 1, i)]);
+      const V c = ldv<LM>(&p[idx(mu, par, 2, i)]);
+      u.e[0][0] = mk<R>(R(a.x), R(a.y));
+      u.e[0][1] = mk<R>(R(a.z), R(a.w));
+      u.e[0][2] = mk<R>(R(b.x), R(b.y));
+      u.e[1][0] = mk<R>(R(b.z), R(b.w));
+      u.e[1][1] = mk<R>(R(c.x), R(c.y));
+      u.e[1][2] = mk<R>(R(c.z), R(c.w));
+    } else {
+      // 2-component chunks: chunk c = element c of the row-major 3x3.
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const V v = ldv<LM>(&p[idx(mu, par, c, i)]);
+        u.e[c / 3][c % 3] = mk<R>(R(v.x), R(v.y));
+      }
+    }
+    if (NR == 12) reconstruct_row2(u);
+    return u;
+  }
+
   template <typename R>
-  __device__ __forceinline__ void store(int mu, int par, uint32_t i, const m3<R>& u) const;
+  __device__ __forceinline__ void store(int mu, int par, uint32_t i, const m3<R>& u) const {
+    if constexpr (sizeof(V) == 4 * sizeof(S)) {
+      V a, b, c;
+      a.x = S(u.e[0][0].re), a.y = S(u.e[0][0].im), a.z = S(u.e[0][1].re), a.w = S(u.e[0][1].im);
+      b.x = S(u.e[0][2].re), b.y = S(u.e[0][2].im), b.z = S(u.e[1][0].re), b.w = S(u.e[1][0].im);
+      c.x = S(u.e[1][1].re), c.y = S(u.e[1][1].im), c.z = S(u.e[1][2].re), c.w = S(u.e[1][2].im);
+      p[idx(mu, par, 0, i)] = a;
+      p[idx(mu, par, 1, i)] = b;
+      p[idx(mu, par, 2, i)] = c;
+    } else {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        V v;
+        v.x = S(u.e[c / 3][c % 3].re);
+        v.y = S(u.e[c / 3][c % 3].im);
+        p[idx(mu, par, c, i)] = v;
+      }
+    }
+  }
 };
-
-// 2-component chunks: chunk c = element c of the row-major 3x3 (rows 0..NR/6-1).
-template <typename S, int NR, typename R>
-__device__ __forceinline__ m3<R> load2(const Links<S, NR>& f, int mu, int par, uint32_t i) {
-  m3<R> u;
-#pragma unroll
-  for (int c = 0; c < Links<S, NR>::NC; ++c) {
-    auto v = __ldg(&f.p[f.idx(mu, par, c, i)]);
-    u.e[c / 3][c % 3] = mk<R>(R(v.x), R(v.y));
-  }
-  if (NR == 12) reconstruct_row2(u);
-  return u;
-}
-template <typename S, int NR, typename R>
-__device__ __forceinline__ void store2(const Links<S, NR>& f, int mu, int par, uint32_t i, const m3<R>& u) {
-#pragma unroll
-  for (int c = 0; c < Links<S, NR>::NC; ++c) {
-    typename Links<S, NR>::V v;
-    v.x = S(u.e[c / 3][c % 3].re);
-    v.y = S(u.e[c / 3][c % 3].im);
-    f.p[f.idx(mu, par, c, i)] = v;
-  }
-}
-
-template <>
-template <typename R>
-__device__ __forceinline__ m3<R> Links<double, 18>::load(int mu, int par, uint32_t i) const {
-  return load2<double, 18, R>(*this, mu, par, i);
-}
-template <>
-template <typename R>
-__device__ __forceinline__ m3<R> Links<double, 12>::load(int mu, int par, uint32_t i) const {
-  return load2<double, 12, R>(*this, mu, par, i);
-}
-template <>
-template <typename R>
-__device__ __forceinline__ m3<R> Links<float, 18>::load(int mu, int par, uint32_t i) const {
-  return load2<float, 18, R>(*this, mu, par, i);
-}
-template <>
-template <typename R>
-__device__ __forceinline__ void Links<double, 18>::store(int mu, int par, uint32_t i, const m3<R>& u) const {
-  store2<double, 18, R>(*this, mu, par, i, u);
-}
-template <>
-template <typename R>
-__device__ __forceinline__ void Links<double, 12>::store(int mu, int par, uint32_t i, const m3<R>& u) const {
-  store2<double, 12, R>(*this, mu, par, i, u);
-}
-template <>
-template <typename R>
-__device__ __forceinline__ void Links<float, 18>::store(int mu, int par, uint32_t i, const m3<R>& u) const {
-  store2<float, 18, R>(*this, mu, par, i, u);
-}
-
-// FP32 12-real: three float4 chunks (e00,e01), (e02,e10), (e11,e12).
-template <>
-template <typename R>
-__device__ __forceinline__ m3<R> Links<float, 12>::load(int mu, int par, uint32_t i) const {
-  float4 a = __ldg(&p[idx(mu, par, 0, i)]);
-  float4 b = __ldg(&p[idx(mu, par, 1, i)]);
-  float4 c = __ldg(&p[idx(mu, par, 2, i)]);
-  m3<R> u;
-  u.e[0][0] = mk<R>(R(a.x), R(a.y));
-  u.e[0][1] = mk<R>(R(a.z), R(a.w));
-  u.e[0][2] = mk<R>(R(b.x), R(b.y));
-  u.e[1][0] = mk<R>(R(b.z), R(b.w));
-  u.e[1][1] = mk<R>(R(c.x), R(c.y));
-  u.e[1][2] = mk<R>(R(c.z), R(c.w));
-  reconstruct_row2(u);
-  return u;
-}
-template <>
-template <typename R>
-__device__ __forceinline__ void Links<float, 12>::store(int mu, int par, uint32_t i, const m3<R>& u) const {
-  p[idx(mu, par, 0, i)] = make_float4(float(u.e[0][0].re), float(u.e[0][0].im), float(u.e[0][1].re),
-                                      float(u.e[0][1].im));
-  p[idx(mu, par, 1, i)] = make_float4(float(u.e[0][2].re), float(u.e[0][2].im), float(u.e[1][0].re),
-                                      float(u.e[1][0].im));
-  p[idx(mu, par, 2, i)] = make_float4(float(u.e[1][1].re), float(u.e[1][1].im), float(u.e[1][2].re),
-                                      float(u.e[1][2].im));
-}
 
 // ---- su(3) algebra field (flow accumulator): 8 reals per link --------------------------
 template <typename S>
@@ -220,7 +191,7 @@ struct AlgStore<float> {
   static constexpr int NC = 2;
 };
 
-template <typename S>
+template <typename S, int LM = LD_RO>
 struct AlgField {
   typedef typename AlgStore<S>::V V;
   static constexpr int NC = AlgStore<S>::NC;
@@ -235,7 +206,7 @@ struct AlgField {
     const S* q;
     V v[NC];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) v[c] = p[idx(mu, par, c, i)];
+    for (int c = 0; c < NC; ++c) v[c] = (LM == LD_RO) ? p[idx(mu, par, c, i)] : __ldcg(&p[idx(mu, par, c, i)]);
     q = reinterpret_cast<const S*>(v);
 #pragma unroll
     for (int k = 0; k < 8; ++k) z.a[k] = R(q[k]);

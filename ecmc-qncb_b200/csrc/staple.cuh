@@ -11,9 +11,8 @@
 
 namespace qcb {
 
-template <typename S, int NR, typename R, int MU>
-__device__ __forceinline__ m3<R> staple_sum(const Geom& g, const Links<S, NR>& f, const Coord& x, int par,
-                                            uint32_t i) {
+template <typename F, typename R, int MU>
+__device__ __forceinline__ m3<R> staple_sum(const Geom& g, const F& f, const Coord& x, int par, uint32_t i) {
   m3<R> A;
   set_zero(A);
   const int opp = par ^ 1;
@@ -36,6 +35,62 @@ __device__ __forceinline__ m3<R> staple_sum(const Geom& g, const Links<S, NR>& f
       const uint32_t xmnu = nb_full(g, x, nu, -1);
       m3<R> V0 = f.template load<R>(nu, par, cb_index(xmunu));
       m3<R> V1 = f.template load<R>(MU, opp, cb_index(xmnu));
+      m3<R> T = mul_aa(V0, V1);
+      m3<R> V2 = f.template load<R>(nu, opp, cb_index(xmnu));
+      acc_nn(A, T, V2);
+    }
+  }
+  return A;
+}
+
+// Neighbour offsets of site x in every direction: up[d] = full-index step to x + d,
+// dn[d] = step to x - d (periodic).
+struct NbOff {
+  int32_t up[4], dn[4];
+};
+__device__ __forceinline__ NbOff nb_offsets(const Geom& g, const Coord& x) {
+  NbOff o;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    o.up[d] = (x.c[d] + 1 == g.L[d]) ? (1 - g.L[d]) * g.str[d] : g.str[d];
+    o.dn[d] = (x.c[d] == 0) ? (g.L[d] - 1) * g.str[d] : -g.str[d];
+  }
+  return o;
+}
+__device__ __forceinline__ int32_t sel4(const int32_t* v, int k) {
+  return k == 0 ? v[0] : (k == 1 ? v[1] : (k == 2 ? v[2] : v[3]));
+}
+
+// Same staple sum with the direction mu known only at run time: one code path for all
+// four directions (a quarter of the code of the four MU instantiations), for kernels in
+// which neighbouring blocks handle different directions.
+template <typename F, typename R>
+__device__ __forceinline__ m3<R> staple_sum_rt(const Geom& g, const F& f, const Coord& x, int mu, int par,
+                                               uint32_t i) {
+  m3<R> A;
+  set_zero(A);
+  const int opp = par ^ 1;
+  const NbOff o = nb_offsets(g, x);
+  const int32_t upmu = sel4(o.up, mu);
+  const uint32_t xmu = (uint32_t)((int32_t)x.s + upmu);
+#pragma unroll
+  for (int nu = 0; nu < 4; ++nu) {
+    if (nu == mu) continue;
+    {
+      // forward: U_nu(x+mu) U_mu(x+nu)^dagger U_nu(x)^dagger
+      const uint32_t xnu = (uint32_t)((int32_t)x.s + o.up[nu]);
+      m3<R> U0 = f.template load<R>(nu, opp, cb_index(xmu));
+      m3<R> U1 = f.template load<R>(mu, opp, cb_index(xnu));
+      m3<R> T = mul_na(U0, U1);
+      m3<R> U2 = f.template load<R>(nu, par, i);
+      acc_na(A, T, U2);
+    }
+    {
+      // backward: U_nu(x+mu-nu)^dagger U_mu(x-nu)^dagger U_nu(x-nu)
+      const uint32_t xmunu = (uint32_t)((int32_t)x.s + upmu + o.dn[nu]);
+      const uint32_t xmnu = (uint32_t)((int32_t)x.s + o.dn[nu]);
+      m3<R> V0 = f.template load<R>(nu, par, cb_index(xmunu));
+      m3<R> V1 = f.template load<R>(mu, opp, cb_index(xmnu));
       m3<R> T = mul_aa(V0, V1);
       m3<R> V2 = f.template load<R>(nu, opp, cb_index(xmnu));
       acc_nn(A, T, V2);

@@ -210,14 +210,16 @@ __device__ __forceinline__ void reconstruct_row2(m3<R>& u) {
   u.e[2][2] = conj(u.e[0][0] * u.e[1][1] - u.e[0][1] * u.e[1][0]);
 }
 
-// Gram-Schmidt on rows 0 and 1, then row 2 = conj(row0 x row1).  Arithmetic in R2
-// (double when called from the FP32 path's reunitarisation).
+__device__ __forceinline__ double rsqrt_r(double x) { return 1.0 / sqrt(x); }
+__device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
+
+// Gram-Schmidt on rows 0 and 1, then row 2 = conj(row0 x row1), in the arithmetic of R.
 template <typename R>
 __device__ __forceinline__ void reunitarize_rows(m3<R>& u) {
   R n0 = 0;
 #pragma unroll
   for (int j = 0; j < 3; ++j) n0 += u.e[0][j].re * u.e[0][j].re + u.e[0][j].im * u.e[0][j].im;
-  R inv0 = R(1) / sqrt(n0);
+  R inv0 = rsqrt_r(n0);
 #pragma unroll
   for (int j = 0; j < 3; ++j) u.e[0][j] = inv0 * u.e[0][j];
   // <r0, r1> = sum conj(r0_j) r1_j
@@ -229,7 +231,7 @@ __device__ __forceinline__ void reunitarize_rows(m3<R>& u) {
   R n1 = 0;
 #pragma unroll
   for (int j = 0; j < 3; ++j) n1 += u.e[1][j].re * u.e[1][j].re + u.e[1][j].im * u.e[1][j].im;
-  R inv1 = R(1) / sqrt(n1);
+  R inv1 = rsqrt_r(n1);
 #pragma unroll
   for (int j = 0; j < 3; ++j) u.e[1][j] = inv1 * u.e[1][j];
   reconstruct_row2(u);

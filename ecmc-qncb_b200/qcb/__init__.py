@@ -30,9 +30,9 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import FP32, FP64, R12, R18, HbParams, QcbError, check, lib
+from ._lib import FP32, FP64, R12, R18, BatchPlan, HbParams, QcbError, check, lib
 
-__all__ = ["Context", "GaugeField", "PhiloxStream", "GradientFlow", "HbParams", "QcbError", "heatbathcb",
+__all__ = ["Context", "GaugeField", "Batch", "BatchPlan", "PhiloxStream", "GradientFlow", "HbParams", "QcbError", "heatbathcb",
            "observables", "io", "save_ildg_clime", "read_ildg_clime", "FP32", "FP64", "R12", "R18",
            "device_count"]
 
@@ -164,6 +164,84 @@ class GaugeField:
     def close(self) -> None:
         if getattr(self, "h", None):
             lib().qcb_lattice_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many lattices advanced by one persistent launch per phase (qcb_batch).  Borrows the
+    fields, which must outlive it."""
+
+    def __init__(self, ctx: Context, fields):
+        self.ctx = ctx
+        self.fields = list(fields)
+        arr = (C.c_void_p * len(self.fields))(*[f.h.value for f in self.fields])
+        h = C.c_void_p()
+        check(lib().qcb_batch_create(ctx.h, len(self.fields), arr, C.byref(h)))
+        self.h = h
+
+    @property
+    def n(self) -> int:
+        return len(self.fields)
+
+    @staticmethod
+    def _u64(v):
+        return (C.c_uint64 * len(v))(*[int(x) for x in v])
+
+    @staticmethod
+    def _f64(v):
+        return (C.c_double * len(v))(*[float(x) for x in v])
+
+    def set_tiles(self, hb=None, flow=None) -> None:
+        mk = lambda v: None if v is None else (C.c_int * self.n)(*v)  # noqa: E731
+        check(lib().qcb_batch_set_tiles(self.h, mk(hb), mk(flow)))
+
+    def tiles(self):
+        hb, fl = (C.c_int * self.n)(), (C.c_int * self.n)()
+        check(lib().qcb_batch_get_tiles(self.h, hb, fl))
+        return list(hb), list(fl)
+
+    def heatbath(self, betas, n_sweeps, n_hits, seeds, sweep_offsets) -> None:
+        check(lib().qcb_batch_heatbath(self.h, self._f64(betas), int(n_sweeps), int(n_hits), self._u64(seeds),
+                                       self._u64(sweep_offsets)))
+
+    def flow_steps(self, eps, n) -> None:
+        check(lib().qcb_batch_flow_steps(self.h, float(eps), int(n)))
+
+    def plaquette(self) -> np.ndarray:
+        out = np.zeros(self.n)
+        check(lib().qcb_batch_plaquette(self.h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def topo_qe(self):
+        q, e = np.zeros(self.n), np.zeros(self.n)
+        check(lib().qcb_batch_topo_qe(self.h, q.ctypes.data_as(C.POINTER(C.c_double)),
+                                      e.ctypes.data_as(C.POINTER(C.c_double))))
+        return q, e
+
+    def run(self, betas, seeds, sweep_offsets, n_sweeps, n_hits=1, eps=0.02, n_groups=0, rk_per_group=0):
+        """Graph-captured workload; returns (plaquette[n], records[n, n_groups+1, 3], used_graph)."""
+        plan = BatchPlan(int(n_sweeps), int(n_hits), float(eps), int(n_groups), int(rk_per_group))
+        per = 1 + 3 * (n_groups + 1)
+        out = np.zeros(self.n * per)
+        used = C.c_int()
+        check(lib().qcb_batch_run(self.h, C.byref(plan), self._f64(betas), self._u64(seeds),
+                                  self._u64(sweep_offsets), out.ctypes.data_as(C.POINTER(C.c_double)),
+                                  C.byref(used)))
+        out = out.reshape(self.n, per)
+        return out[:, 0].copy(), out[:, 1:].reshape(self.n, n_groups + 1, 3), bool(used.value)
+
+    def autotune(self, cache_path=None) -> None:
+        check(lib().qcb_batch_autotune(self.h, None if cache_path is None else os.fsencode(cache_path)))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().qcb_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -25,6 +25,12 @@ class QcbError(RuntimeError):
         self.code = code
 
 
+class BatchPlan(C.Structure):
+    """qcb_batch_plan."""
+    _fields_ = [("n_sweeps", C.c_int), ("n_hits", C.c_int), ("eps", C.c_double), ("n_groups", C.c_int),
+                ("rk_per_group", C.c_int)]
+
+
 class HbParams(C.Structure):
     """qcb_hb_params: RunParamsHbCB of the reference (src/io/params.h:46-63)."""
     _fields_ = [("L_core", C.c_int), ("n_core_dims", C.c_int), ("cold_start", C.c_int),
@@ -77,6 +83,17 @@ SIGNATURES = {
     "qcb_flow_measure": (C.c_int, [_vp, C.c_double, C.c_int, C.c_int, _dp]),
     "qcb_flow_steps": (C.c_int, [_vp, C.c_double, C.c_int]),
     "qcb_plaquette_noalloc": (C.c_int, [_vp, _ip, C.c_int, C.c_int, C.c_size_t, _vp, _vp]),
+    "qcb_batch_create": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "qcb_batch_destroy": (C.c_int, [_vp]),
+    "qcb_batch_set_tiles": (C.c_int, [_vp, _ip, _ip]),
+    "qcb_batch_get_tiles": (C.c_int, [_vp, _ip, _ip]),
+    "qcb_batch_heatbath": (C.c_int, [_vp, _dp, C.c_int, C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "qcb_batch_flow_steps": (C.c_int, [_vp, C.c_double, C.c_int]),
+    "qcb_batch_plaquette": (C.c_int, [_vp, _dp]),
+    "qcb_batch_topo_qe": (C.c_int, [_vp, _dp, _dp]),
+    "qcb_batch_run": (C.c_int, [_vp, C.POINTER(BatchPlan), _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _dp,
+                                _ip]),
+    "qcb_batch_autotune": (C.c_int, [_vp, C.c_char_p]),
     "qcb_params_default": (C.c_int, [C.POINTER(HbParams)]),
     "qcb_params_load": (C.c_int, [C.c_char_p, C.POINTER(HbParams)]),
 }

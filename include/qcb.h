@@ -160,6 +160,49 @@ int qcb_flow_measure(qcb_lattice* lat, double eps, int n_steps_gf, int n_rk_step
 /* n RK3 steps of size eps applied to the lattice in place (no measurement). */
 int qcb_flow_steps(qcb_lattice* lat, double eps, int n);
 
+/* ---- batches of lattices ------------------------------------------------------------
+ * No single counterpart in the reference (it runs one lattice per process,
+ * src/bin/gauge_hb_ncb.cpp:18-201).  A batch advances many independent lattices of any
+ * sizes (same context, precision and storage) in one persistent cooperative launch per
+ * phase: work items (lattice, level, tile of sites) run level-major, each lattice's levels
+ * in order, different lattices overlapping.  Every result is bit-identical to running the
+ * lattice alone through qcb_heatbath / qcb_flow_steps with the same seed and sweep counter.
+ * The batch borrows the lattices: they must outlive it. */
+typedef struct qcb_batch qcb_batch;
+int qcb_batch_create(qcb_ctx* ctx, int n, qcb_lattice* const* lats, qcb_batch** out);
+int qcb_batch_destroy(qcb_batch* b);
+/* Sites per work item for the heatbath / flow of each lattice (multiples of 32 in
+ * [32, 65536]); NULL keeps the current value (default 256). */
+int qcb_batch_set_tiles(qcb_batch* b, const int* hb_tile, const int* flow_tile);
+int qcb_batch_get_tiles(qcb_batch* b, int* hb_tile, int* flow_tile);
+/* n_sweeps checkerboard sweeps of every lattice l at betas[l], seeds[l], sweeps
+ * sweep_offsets[l] .. sweep_offsets[l] + n_sweeps - 1 (one launch).  Asynchronous. */
+int qcb_batch_heatbath(qcb_batch* b, const double* betas, int n_sweeps, int n_hits, const uint64_t* seeds,
+                       const uint64_t* sweep_offsets);
+/* n RK3 steps of size eps on every lattice, in place (one launch). */
+int qcb_batch_flow_steps(qcb_batch* b, double eps, int n_steps);
+/* Per-lattice mean plaquette / clover (Q, E) of every lattice (one launch each). */
+int qcb_batch_plaquette(qcb_batch* b, double* out);
+int qcb_batch_topo_qe(qcb_batch* b, double* q, double* e);
+/* A whole batched workload as one CUDA graph: n_sweeps heatbath sweeps in place, the mean
+ * plaquette, then the Wilson flow on copies of the links with (t, Q, E) recorded before
+ * each of n_groups groups of rk_per_group RK3 steps and once after the last group.
+ * results holds n * (1 + 3 * (n_groups + 1)) doubles: per lattice the plaquette, then the
+ * records.  The graph is captured on the first call with a given plan and replayed after;
+ * *used_graph (if not NULL) tells whether the graph path ran. */
+typedef struct qcb_batch_plan {
+  int n_sweeps, n_hits;
+  double eps;
+  int n_groups, rk_per_group;
+} qcb_batch_plan;
+int qcb_batch_run(qcb_batch* b, const qcb_batch_plan* plan, const double* betas, const uint64_t* seeds,
+                  const uint64_t* sweep_offsets, double* results, int* used_graph);
+/* Project-written autotuner: for each distinct lattice size of the batch, times the
+ * heatbath and the flow of that size's lattices on scratch copies for candidate tiles and
+ * keeps the fastest; results are cached in the JSON file cache_path (created if absent,
+ * NULL = no cache) under keys "<device name>|<precision>-<storage>|<hb|flow>|LxLyLzLt". */
+int qcb_batch_autotune(qcb_batch* b, const char* cache_path);
+
 /* ---- input file ----------------------------------------------------------------------
  * io::load_params(..., RunParamsHbCB&) (src/io/io.cpp:353-399) with the defaults of
  * src/io/params.h:46-63.  Host-only.  Strings are NUL-terminated and truncated to fit. */

@@ -2,6 +2,7 @@
 input-file parser and the ILDG container probe (no kernel launches)."""
 import ctypes as C
 import re
+import sys
 from pathlib import Path
 
 import pytest
@@ -152,3 +153,20 @@ def test_ildg_probe(tmp_path):
     with pytest.raises(qcb.QcbError) as e:
         qcb.io.ildg_probe(tmp_path / "nope")
     assert e.value.code == 3
+
+
+def test_driver_rejects_bad_input(tmp_path):
+    """The drop-in driver reports input errors before touching the GPU (io.cpp:454-461)."""
+    import subprocess
+
+    driver = ROOT / "ecmc-qncb_b200" / "bin" / "gauge_hb_ncb"
+    if not driver.exists():
+        subprocess.run([sys.executable, str(ROOT / "ecmc-qncb_b200" / "build.py")], check=True)
+    bad = tmp_path / "bad.txt"
+    bad.write_text("L_core = eight\n")
+    r = subprocess.run([str(driver), str(bad)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "Error reading input" in r.stderr
+    r = subprocess.run([str(driver), str(tmp_path / "missing.txt")], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "Can't open file" in r.stderr
+    r = subprocess.run([str(driver)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "Usage" in r.stderr

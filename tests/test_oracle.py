@@ -173,3 +173,21 @@ def test_ildg_codec_roundtrip(orc, tmp_path):
     assert np.array_equal(orc.read_ildg(p, dims), u)
     with pytest.raises(ValueError):
         orc.read_ildg(p, (4, 4, 4, 4))
+
+
+def test_checkerboard_schedule_matches_reference_schedule_statistically(orc):
+    """The library's schedule (checkerboard passes, Philox) restated in the oracle samples
+    the same mean plaquette as the reference's (frozen links + random shifts, mt19937_64)
+    on a 4^4 lattice at beta = 6.0."""
+    from stats import binned_mean_err, z_score
+
+    dims = (4, 4, 4, 4)
+    u = orc.hot_philox(dims, 17)
+    cb = []
+    for s in range(2400):
+        u, fails = orc.heatbath_cb(u, dims, 6.0, 1, 1, 99, s)
+        cb.append(orc.plaquette(u, dims))
+    ref = orc.RefChain(4, 4242, False).run(6.0, 2400)
+    z = z_score(cb[200:], ref[200:])
+    print("cb", binned_mean_err(cb[200:]), "ref", binned_mean_err(ref[200:]), "z", z)
+    assert z < 3.0
