@@ -279,6 +279,11 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
+    if not args.no_extra and world == 1:
+        result["batch"] = batch_section(ctx, lib, stream)
+        result["serving"] = serving_section(ctx)
+        result["latency"] = {"p50_s": result["serving"]["p50_s"], "p99_s": result["serving"]["p99_s"],
+                             "workload": "serving stream (config 4)"}
     return result
 
 
@@ -302,6 +307,140 @@ def profile_steps(args) -> int:
         counts.append(ctx.launches() - n0)
     print(json.dumps({"profile": args.storage, "launches_per_step": counts}))
     return 0
+
+
+# ---------------------------------------------------------------------------------------
+def batch_section(ctx, lib, stream):
+    """Batching workload: 64 independent lattices, sizes uniform over {8,12,16,20,24}^4,
+    beta uniform over {5.7, 5.85, 6.0, 6.2} (host seed 2024), alternating hot and cold
+    starts, 100 heatbath sweeps then the flow to t = 2 (100 RK3 steps, Q/E every 0.2), FP32
+    12-real with FP64 reductions; one graph-captured persistent plan; tiles autotuned."""
+    import numpy as np
+    import torch
+
+    import qcb
+
+    rng = np.random.default_rng(2024)
+    n = 64
+    sizes = rng.choice([8, 12, 16, 20, 24], size=n)
+    betas = rng.choice([5.7, 5.85, 6.0, 6.2], size=n)
+    seeds = [3000 + k for k in range(n)]
+    fields = []
+    for k in range(n):
+        f = qcb.GaugeField(ctx, (int(sizes[k]),) * 4, "fp32", 12)
+        if k % 2 == 0:
+            f.hot_start(seeds[k])
+        fields.append(f)
+    vols = [int(L) ** 4 for L in sizes]
+    batch = qcb.Batch(ctx, fields)
+    t0 = time.perf_counter()
+    batch.autotune(os.path.join(os.environ.get("TMPDIR", "/tmp"), "qcb_tune.json"))
+    tune_s = time.perf_counter() - t0
+    hb_tiles, flow_tiles = batch.tiles()
+
+    def timed(fn, reps=2):
+        fn()  # capture / warm
+        ctx.sync()
+        best = 1e30
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            out = fn()
+            b.record(stream)
+            b.synchronize()
+            best = min(best, a.elapsed_time(b))
+        return best, out
+
+    offs = [0] * n
+    hb_ms, _ = timed(lambda: batch.run(betas, seeds, offs, n_sweeps=100, n_groups=0, rk_per_group=0))
+    fl_ms, _ = timed(lambda: batch.run(betas, seeds, offs, n_sweeps=0, eps=0.02, n_groups=10, rk_per_group=10))
+    all_ms, (plaq, rec, used) = timed(lambda: batch.run(betas, seeds, offs, n_sweeps=100, eps=0.02, n_groups=10,
+                                                         rk_per_group=10))
+    updates = 100 * 4 * sum(vols)
+    site_steps = 100 * sum(vols)
+    # the same heatbath work through per-lattice calls (one launch per pass and lattice)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for k, f in enumerate(fields):
+        qcb._lib.check(lib.qcb_heatbath(f.h, float(betas[k]), 100, 1, seeds[k], 0))
+    b.record(stream)
+    b.synchronize()
+    single_ms = a.elapsed_time(b)
+    batch.close()
+    return {"workload": "64 lattices {8..24}^4 x {5.7..6.2}, 100 sweeps + flow to t=2, fp32-12", "graph": used,
+            "total_volume": sum(vols), "ms_per_plan": all_ms,
+            "hb": {"value": updates / (hb_ms / 1e3), "unit": "link-updates/s", "ms": hb_ms},
+            "flow": {"value": site_steps / (fl_ms / 1e3), "unit": "site-steps/s", "ms": fl_ms},
+            "unbatched_hb": {"value": updates / (single_ms / 1e3), "unit": "link-updates/s", "ms": single_ms,
+                             "launches": 64 * 800},
+            "autotune_s": tune_s, "tiles": {"hb": sorted(set(hb_tiles)), "flow": sorted(set(flow_tiles))},
+            "mean_plaquette": float(np.mean(plaq)), "mean_E_t2": float(np.mean(rec[:, -1, 2]))}
+
+
+def serving_section(ctx, n_requests=100, rate=20.0):
+    """Serving workload: a Poisson stream (mean `rate` req/s, stream seed 77) of 70% Wilson-flow
+    measurements to t ~ U[1, 6] and 30% generate-N-sweeps jobs with N ~ U[10, 200]; sizes
+    16^4 (0.4), 24^4 (0.3), 32^4 (0.2), 48^4 (0.1); beta ~ U[5.8, 6.3]; FP32 12-real.  The
+    inputs are pre-thermalised on the device from per-request seeds before the stream starts
+    (untimed setup) and stay resident.  Latency = completion - arrival on the server clock."""
+    import threading
+
+    import numpy as np
+
+    import qcb
+
+    rng = np.random.default_rng(77)
+    gaps = rng.exponential(1.0 / rate, size=n_requests)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    kinds = rng.random(n_requests) < 0.7
+    sizes = rng.choice([16, 24, 32, 48], p=[0.4, 0.3, 0.2, 0.1], size=n_requests)
+    betas = rng.uniform(5.8, 6.3, size=n_requests)
+    tflow = rng.uniform(1.0, 6.0, size=n_requests)
+    nsw = rng.integers(10, 201, size=n_requests)
+    lib = qcb._lib.lib()
+    fields = []
+    for k in range(n_requests):
+        f = qcb.GaugeField(ctx, (int(sizes[k]),) * 4, "fp32", 12)
+        f.hot_start(7000 + k)
+        qcb._lib.check(lib.qcb_heatbath(f.h, float(betas[k]), 20, 1, 7000 + k, 0))
+        fields.append(f)
+    ctx.sync()
+    srv = qcb.Server(ctx, "fp32", 12, hbm_budget=48 << 30, quantum_sweeps=2, quantum_steps=4)
+    submit_t = {}
+
+    def feeder():
+        t_start = time.perf_counter()
+        for k in range(n_requests):
+            wait = arrivals[k] - (time.perf_counter() - t_start)
+            if wait > 0:
+                time.sleep(wait)
+            if kinds[k]:
+                jid = srv.submit_flow(fields[k], 0.02, int(round(tflow[k] / 0.02)))
+            else:
+                jid = srv.submit_sweeps(fields[k], float(betas[k]), int(nsw[k]), seed=7000 + k, sweep_offset=20)
+            submit_t[jid] = k
+
+    th = threading.Thread(target=feeder)
+    th.start()
+    th.join()
+    srv.drain(3600)
+    res = srv.poll(n_requests + 10)
+    stats = srv.stats()
+    srv.close()
+    lat = np.array([r.finish_s - r.submit_s for r in res])
+    wait = np.array([r.admit_s - r.submit_s for r in res])
+    ok = all(r.status == 0 for r in res)
+    span = max(r.finish_s for r in res) - min(r.submit_s for r in res)
+    work_sites = sum((round(tflow[k] / 0.02) if kinds[k] else 0) * int(sizes[k]) ** 4 for k in range(n_requests))
+    work_upd = sum((0 if kinds[k] else int(nsw[k])) * 4 * int(sizes[k]) ** 4 for k in range(n_requests))
+    return {"workload": f"Poisson {rate} req/s, {n_requests} requests, 70% flow t~U[1,6], 30% N~U[10,200] sweeps, "
+                        "sizes 16/24/32/48^4 (0.4/0.3/0.2/0.1), beta~U[5.8,6.3], fp32-12",
+            "all_ok": ok, "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "admission_wait_p99_s": float(np.percentile(wait, 99)),
+            "throughput_jobs_per_s": len(res) / span, "span_s": span,
+            "flow_site_steps_per_s": work_sites / span, "hb_link_updates_per_s": work_upd / span,
+            "offered_flow_site_steps": work_sites, "offered_link_updates": work_upd,
+            "ticks": stats["ticks"], "max_active": stats["max_active"], "arena_peak_bytes": stats["arena_peak"]}
 
 
 # ---------------------------------------------------------------------------------------
@@ -350,6 +489,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batching and serving sections")
     ap.add_argument("--profile", action="store_true",
                     help="run only warmup + steps of the workload (for ncu); print launch counts")
     ap.add_argument("--storage", choices=["fp32-12", "fp64-18"], default="fp32-12")

@@ -180,8 +180,10 @@ int qcb_ctx_create(int device, unsigned flags, qcb_ctx** out) {
   return QCB_OK;
 }
 
-int qcb_ctx_destroy(qcb_ctx* c) {
-  if (!c) return QCB_OK;
+}  // extern "C"
+
+namespace {
+void ctx_free(qcb_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   cudaFree(c->d_status);
@@ -195,6 +197,36 @@ int qcb_ctx_destroy(qcb_ctx* c) {
   if (c->stream) cudaStreamDestroy(c->stream);
   cudaGetLastError();
   delete c;
+}
+}  // namespace
+
+void qcb::ctx_ref(qcb_ctx* c) {
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->refs++;
+}
+
+void qcb::ctx_unref(qcb_ctx* c) {
+  bool free_now = false;
+  {
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->refs--;
+    free_now = c->doomed && c->refs == 0;
+  }
+  if (free_now) ctx_free(c);
+}
+
+extern "C" {
+
+int qcb_ctx_destroy(qcb_ctx* c) {
+  if (!c) return QCB_OK;
+  {
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (c->refs > 0) {
+      c->doomed = true;  // freed by the last child's destroy
+      return QCB_OK;
+    }
+  }
+  ctx_free(c);
   return QCB_OK;
 }
 
@@ -254,6 +286,7 @@ int qcb_lattice_create(qcb_ctx* c, const int dims[4], int precision, int storage
   CU(cudaMemsetAsync(L->dev.links, 0, L->bytes, c->stream), "memset");
   CU(launch_cold(L->dev, c->stream, 0), "cold start");
   c->launches++;
+  c->refs++;  // under the context lock
   *out = L;
   return QCB_OK;
 }
@@ -272,6 +305,7 @@ int qcb_lattice_destroy(qcb_lattice* L) {
     cudaGetLastError();
   }
   delete L;
+  ctx_unref(c);
   return QCB_OK;
 }
 

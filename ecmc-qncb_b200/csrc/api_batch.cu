@@ -272,6 +272,8 @@ int enqueue_plan(qcb_batch* b, const qcb_batch_plan& p) {
   return QCB_OK;
 }
 
+void batch_free(qcb_batch* b);
+
 bool same_plan(const qcb_batch_plan& a, const qcb_batch_plan& c) {
   return a.n_sweeps == c.n_sweeps && a.n_hits == c.n_hits && a.eps == c.eps && a.n_groups == c.n_groups &&
          a.rk_per_group == c.rk_per_group;
@@ -302,7 +304,8 @@ int qcb_batch_create(qcb_ctx* ctx, int n, qcb_lattice* const* lats, qcb_batch** 
   b->hb_tile.assign(n, DEFAULT_TILE);
   b->flow_tile.assign(n, DEFAULT_TILE);
   auto fail_all = [&](int code) {
-    qcb_batch_destroy(b);
+    b->ctx = nullptr;  // not counted yet
+    batch_free(b);
     return code;
   };
   for (int l = 0; l < n; ++l) {
@@ -323,14 +326,25 @@ int qcb_batch_create(qcb_ctx* ctx, int n, qcb_lattice* const* lats, qcb_batch** 
   int r = upload_layout(b);
   if (r == QCB_OK) r = upload_flow_desc(b);
   if (r != QCB_OK) return fail_all(r);
+  ctx->refs++;  // under the context lock
   *out = b;
   return QCB_OK;
 }
 
 int qcb_batch_destroy(qcb_batch* b) {
   if (!b) return QCB_OK;
-  cudaSetDevice(b->ctx->device);
-  cudaStreamSynchronize(b->ctx->stream);
+  qcb_ctx* c = b->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  batch_free(b);
+  ctx_unref(c);
+  return QCB_OK;
+}
+
+}  // extern "C"
+
+namespace {
+void batch_free(qcb_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   cudaFree(b->d_desc);
   cudaFreeHost(b->h_desc);
@@ -343,8 +357,10 @@ int qcb_batch_destroy(qcb_batch* b) {
   cudaFreeHost(b->h_out);
   cudaGetLastError();
   delete b;
-  return QCB_OK;
 }
+}  // namespace
+
+extern "C" {
 
 int qcb_batch_set_tiles(qcb_batch* b, const int* hb_tile, const int* flow_tile) {
   if (!b) return bfail(QCB_ERR_INVALID, "null batch");

@@ -20,6 +20,11 @@ struct qcb_ctx {
   double* h_stage = nullptr;  // pinned, for file I/O
   uint64_t launches = 0;
   std::mutex mu;
+  // Objects created on this context (lattices, batches, servers).  qcb_ctx_destroy with
+  // live objects only marks the context; the last object's destroy frees it, so no child
+  // ever uses a freed context.
+  int refs = 0;
+  bool doomed = false;
 };
 
 struct qcb_lattice {
@@ -32,6 +37,9 @@ struct qcb_lattice {
 };
 
 namespace qcb {
+// Reference counting of a context's child objects (see qcb_ctx::refs).
+void ctx_ref(qcb_ctx* c);
+void ctx_unref(qcb_ctx* c);
 // Allocates a lattice's Wilson-flow work space (two link buffers + accumulator) once.
 int ensure_flow_space(qcb_lattice* L);
 // Reads and clears the context's device status words (after synchronising its stream).

@@ -18,6 +18,10 @@ struct BatchLat {
   uint32_t sweep0;  // sweep counter of the launch's first sweep
   uint32_t tile;    // sites per work item (any multiple of the block size)
   uint32_t ntiles;  // work items of this lattice per level (flow: 8 x site tiles)
+  uint32_t nlev;    // levels this lattice takes part in (0 = all levels of the launch)
+  int kind;         // BATCH_HB or BATCH_FLOW (mixed launches); BATCH_NONE: no work
+  int n_hits;       // heatbath hits (0 = the launch's value)
+  double eps;       // flow step (0 = the launch's value)
 };
 
 // One persistent launch: nlevels levels of per_level items each.
@@ -33,10 +37,10 @@ struct BatchRun {
   double eps;
 };
 
-enum : int { BATCH_HB = 0, BATCH_FLOW = 1 };
+enum : int { BATCH_NONE = -1, BATCH_HB = 0, BATCH_FLOW = 1, BATCH_MIXED = 2 };
 
-// Cooperative persistent launch: the grid is the co-resident maximum (capped by
-// max_blocks when > 0) for the given block size.
+// Cooperative persistent launch (kind BATCH_HB, BATCH_FLOW or BATCH_MIXED): the grid is the
+// co-resident maximum (capped by max_blocks when > 0) for the given block size.
 cudaError_t launch_batch(int kind, const BatchRun& run, int prec, int nr, int block, int max_blocks,
                          cudaStream_t s);
 

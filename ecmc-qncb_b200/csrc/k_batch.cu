@@ -89,10 +89,67 @@ __device__ __forceinline__ void block_release(uint32_t* done) {
   if (threadIdx.x == 0) atomicAdd(done, 1u);
 }
 
-// ---- heatbath ------------------------------------------------------------------------
+// ---- one work item ----------------------------------------------------------------------
+// Heatbath level k: pass k % 8 (mu = pass / 2, parity = pass % 2) of sweep sweep0 + k / 8;
+// item tile = a tile of that pass's sites.
 template <typename S, int NR>
-__global__ void __launch_bounds__(128) k_batch_hb(BatchRun run) {
+__device__ __forceinline__ uint32_t hb_item(const BatchRun& run, const BatchLat& B, uint32_t level, uint32_t tile) {
   typedef Links<S, NR, LD_CG> F;
+  const uint32_t sweep = B.sweep0 + level / 8;
+  const int pass = (int)(level & 7), mu = pass >> 1, par = pass & 1;
+  F f;
+  f.p = reinterpret_cast<typename F::V*>(B.links);
+  f.stride = B.g.stride;
+  const S beta = S(B.beta);
+  const int n_hits = B.n_hits > 0 ? B.n_hits : run.n_hits;
+  uint32_t fails = 0;
+  for (uint32_t k = threadIdx.x; k < B.tile; k += blockDim.x) {
+    const uint32_t i = tile * B.tile + k;
+    if (i >= B.g.Vh) break;
+    fails += hb_update_link_rt<F, S, NR>(B.g, f, mu, par, i, beta, B.k0, B.k1, sweep, n_hits);
+  }
+  return fails;
+}
+
+// Flow level j = 3 s + k is stage k of RK3 step s.  With a = links, b = work for even s
+// (swapped for odd s): stage 0 a -> b, stage 1 b -> a, stage 2 a -> b.  A flow item covers a
+// tile of one (mu, parity) block: item r of a lattice -> (mu, parity) = r % 8, tile = r / 8.
+template <typename S, int NR>
+__device__ __forceinline__ void flow_item(const BatchRun& run, const BatchLat& B, uint32_t level, uint32_t local) {
+  typedef Links<S, NR, LD_CG> F;
+  typedef AlgField<S, LD_CG> Z;
+  const uint32_t step = level / 3, stage = level - 3 * step;
+  void* a = (step & 1) ? B.work : B.links;
+  void* bb = (step & 1) ? B.links : B.work;
+  F src, dst;
+  src.p = reinterpret_cast<typename F::V*>(stage == 1 ? bb : a);
+  dst.p = reinterpret_cast<typename F::V*>(stage == 1 ? a : bb);
+  src.stride = dst.stride = B.g.stride;
+  Z acc;
+  acc.p = reinterpret_cast<typename Z::V*>(B.acc);
+  acc.stride = B.g.stride;
+  const int mp8 = (int)(local & 7), mu = mp8 >> 1, par = mp8 & 1;
+  const uint32_t tile = local >> 3;
+  const S eps = S(B.eps != 0.0 ? B.eps : run.eps);
+  for (uint32_t k = threadIdx.x; k < B.tile; k += blockDim.x) {
+    const uint32_t i = tile * B.tile + k;
+    if (i >= B.g.Vh) break;
+    if (stage == 0)
+      flow_link_rt<F, Z, S, 1>(B.g, src, dst, acc, eps, mu, par, i);
+    else if (stage == 1)
+      flow_link_rt<F, Z, S, 2>(B.g, src, dst, acc, eps, mu, par, i);
+    else
+      flow_link_rt<F, Z, S, 3>(B.g, src, dst, acc, eps, mu, par, i);
+  }
+}
+
+// ---- the persistent kernel -----------------------------------------------------------------
+// KINDS: BATCH_HB or BATCH_FLOW for a launch of one kind, BATCH_MIXED when each lattice's
+// descriptor says which kind its items are.  A lattice with B.nlev != 0 takes part in its
+// first B.nlev levels only; its items at later levels are skipped (no wait, no release), and
+// a lattice of kind BATCH_NONE in a mixed launch takes part in none.
+template <typename S, int NR, int KINDS>
+__global__ void __launch_bounds__(128) k_batch(BatchRun run) {
   const uint64_t total = (uint64_t)run.nlevels * run.per_level;
   uint32_t fails = 0;
   for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
@@ -100,73 +157,25 @@ __global__ void __launch_bounds__(128) k_batch_hb(BatchRun run) {
     const uint32_t r = (uint32_t)(item - (uint64_t)level * run.per_level);
     const int l = find_lattice(run.prefix, run.nlat, r);
     const BatchLat& B = run.lats[l];
-    const uint32_t tile = r - run.prefix[l];
+    if (B.nlev != 0 && level >= B.nlev) continue;
+    if (KINDS == BATCH_MIXED && B.kind == BATCH_NONE) continue;
+    const uint32_t local = r - run.prefix[l];
     if (level > 0 && !block_wait(&run.done[l], level * B.ntiles, run.status)) return;
-    const uint32_t sweep = B.sweep0 + level / 8;
-    const int pass = (int)(level & 7), mu = pass >> 1, par = pass & 1;
-    F f;
-    f.p = reinterpret_cast<typename F::V*>(B.links);
-    f.stride = B.g.stride;
-    const S beta = S(B.beta);
-    for (uint32_t k = threadIdx.x; k < B.tile; k += blockDim.x) {
-      const uint32_t i = tile * B.tile + k;
-      if (i >= B.g.Vh) break;
-      fails += hb_update_link_rt<F, S, NR>(B.g, f, mu, par, i, beta, B.k0, B.k1, sweep, run.n_hits);
-    }
+    const int kind = (KINDS == BATCH_MIXED) ? B.kind : KINDS;
+    if (kind == BATCH_HB)
+      fails += hb_item<S, NR>(run, B, level, local);
+    else
+      flow_item<S, NR>(run, B, level, local);
     block_release(&run.done[l]);
   }
   if (fails) atomicAdd(&run.status[0], fails);
 }
 
-// ---- Wilson flow -----------------------------------------------------------------------
-// Level j = 3 s + k is stage k of RK3 step s.  With a = links, b = work for even s (swapped
-// for odd s): stage 0 a -> b, stage 1 b -> a, stage 2 a -> b.  A flow item covers a tile of
-// one (mu, parity) block: item r of a lattice -> (mu, parity) = r % 8, tile = r / 8.  The
-// direction is a run-time value in these kernels (one code path for every mu).
-template <typename S, int NR>
-__global__ void __launch_bounds__(128) k_batch_flow(BatchRun run) {
-  typedef Links<S, NR, LD_CG> F;
-  typedef AlgField<S, LD_CG> Z;
-  const uint64_t total = (uint64_t)run.nlevels * run.per_level;
-  for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
-    const uint32_t level = (uint32_t)(item / run.per_level);
-    const uint32_t r = (uint32_t)(item - (uint64_t)level * run.per_level);
-    const int l = find_lattice(run.prefix, run.nlat, r);
-    const BatchLat& B = run.lats[l];
-    const uint32_t local = r - run.prefix[l];
-    if (level > 0 && !block_wait(&run.done[l], level * B.ntiles, run.status)) return;
-    const uint32_t step = level / 3, stage = level - 3 * step;
-    void* a = (step & 1) ? B.work : B.links;
-    void* b = (step & 1) ? B.links : B.work;
-    F src, dst;
-    src.p = reinterpret_cast<typename F::V*>(stage == 1 ? b : a);
-    dst.p = reinterpret_cast<typename F::V*>(stage == 1 ? a : b);
-    src.stride = dst.stride = B.g.stride;
-    Z acc;
-    acc.p = reinterpret_cast<typename Z::V*>(B.acc);
-    acc.stride = B.g.stride;
-    const int mp8 = (int)(local & 7), mu = mp8 >> 1, par = mp8 & 1;
-    const uint32_t tile = local >> 3;
-    const S eps = S(run.eps);
-    for (uint32_t k = threadIdx.x; k < B.tile; k += blockDim.x) {
-      const uint32_t i = tile * B.tile + k;
-      if (i >= B.g.Vh) break;
-if (stage == 0)
-        flow_link_rt<F, Z, S, 1>(B.g, src, dst, acc, eps, mu, par, i);
-      else if (stage == 1)
-        flow_link_rt<F, Z, S, 2>(B.g, src, dst, acc, eps, mu, par, i);
-      else
-        flow_link_rt<F, Z, S, 3>(B.g, src, dst, acc, eps, mu, par, i);
-
-    }
-    block_release(&run.done[l]);
-  }
-}
-
 // ---- launch -------------------------------------------------------------------------------
 template <typename S, int NR>
 static cudaError_t batch_launch_impl(int kind, const BatchRun& run, int block, int max_blocks, cudaStream_t s) {
-  void* fn = (kind == BATCH_HB) ? (void*)k_batch_hb<S, NR> : (void*)k_batch_flow<S, NR>;
+  void* fn = (kind == BATCH_HB) ? (void*)k_batch<S, NR, BATCH_HB>
+             : (kind == BATCH_FLOW) ? (void*)k_batch<S, NR, BATCH_FLOW> : (void*)k_batch<S, NR, BATCH_MIXED>;
   int per_sm = 0, dev = 0, sms = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0);
   if (e != cudaSuccess) return e;

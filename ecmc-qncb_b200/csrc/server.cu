@@ -1,0 +1,551 @@
+// server.cu — request server with continuous batching (include/qcb.h, "serving").
+//
+// Jobs wait in arrival order; the scheduler thread admits the head job while a job slot is
+// free and the work-space arena (a single device allocation made at creation, the server's
+// HBM budget) has room for it, so later arrivals never overtake earlier ones.  Each tick
+// builds one descriptor per admitted job (a sweeps job advances by quantum_sweeps sweeps, a
+// flow job by quantum_steps RK3 steps, each lattice with its own level count), runs them in
+// one mixed persistent launch, measures the jobs that finished (batched plaquette / clover
+// reductions), copies the results back, and then admits the next arrivals.
+#include <string.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "api_internal.h"
+#include "batch.h"
+
+using namespace qcb;
+
+namespace {
+
+struct Job {
+  uint64_t id;
+  qcb_job spec;
+  cudaEvent_t ready = nullptr;  // lattice ready on the client's stream at submission
+  double submit_s = 0, admit_s = 0;
+  // work space (flow jobs): offsets into the arena
+  size_t ws_off = 0, ws_bytes = 0;
+  void* fw0 = nullptr;
+  void* fw1 = nullptr;
+  void* acc = nullptr;
+  bool started = false;
+  int done_units = 0;  // sweeps or RK3 steps done
+  bool cancel = false;
+};
+
+// First-fit allocator over [0, size) with 256-byte granules.
+class Arena {
+ public:
+  void init(size_t size) {
+    free_[0] = size;
+    size_ = size;
+  }
+  bool alloc(size_t bytes, size_t* off) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= bytes) {
+        *off = it->first;
+        const size_t rest = it->second - bytes, start = it->first + bytes;
+        free_.erase(it);
+        if (rest) free_[start] = rest;
+        used_ += bytes;
+        if (used_ > peak_) peak_ = used_;
+        return true;
+      }
+    }
+    return false;
+  }
+  void release(size_t off, size_t bytes) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    used_ -= bytes;
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  size_t peak() const { return peak_; }
+
+ private:
+  std::map<size_t, size_t> free_;
+  size_t size_ = 0, used_ = 0, peak_ = 0;
+};
+
+uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
+
+}  // namespace
+
+struct qcb_server {
+  qcb_ctx* ctx = nullptr;
+  qcb_server_config cfg{};
+  cudaStream_t stream = nullptr;
+  char* arena_base = nullptr;
+  size_t arena_bytes = 0;
+  Arena arena;
+  std::chrono::steady_clock::time_point t0;
+
+  std::mutex mu;
+  std::condition_variable cv;       // scheduler wake-up
+  std::condition_variable done_cv;  // drain
+  std::deque<Job*> pending;
+  std::vector<Job*> active;
+  std::deque<qcb_job_result> results;
+  uint64_t next_id = 1, submitted = 0, admitted = 0, completed = 0, ticks = 0;
+  int max_active = 0;
+  bool stop = false;
+  std::thread thr;
+
+  // device scratch for one tick
+  BatchLat* d_desc = nullptr;
+  BatchLat* h_desc = nullptr;
+  uint32_t* d_prefix = nullptr;
+  uint32_t* h_prefix = nullptr;
+  uint32_t* d_done = nullptr;
+  uint32_t* d_status = nullptr;
+  uint32_t* h_status = nullptr;
+  double* d_scratch = nullptr;
+  size_t scratch_cap = 0;
+  double* d_out = nullptr;
+  double* h_out = nullptr;
+  int cap = 0;  // descriptor capacity (max_jobs)
+
+  double now() const {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+};
+
+namespace {
+
+size_t ws_bytes_for(const qcb_lattice* L) { return 2 * L->bytes + alg_bytes(L->dev.g, L->dev.prec) + 3 * 256; }
+
+void finish(qcb_server* s, Job* j, int status, double plaq, double t, double q, double e) {
+  qcb_job_result r;
+  memset(&r, 0, sizeof r);
+  r.id = j->id;
+  r.status = status;
+  r.kind = j->spec.kind;
+  r.plaquette = plaq;
+  r.t = t;
+  r.q = q;
+  r.e = e;
+  r.submit_s = j->submit_s;
+  r.admit_s = j->admit_s;
+  r.finish_s = s->now();
+  if (j->ws_bytes) s->arena.release(j->ws_off, j->ws_bytes);
+  if (j->ready) cudaEventDestroy(j->ready);
+  s->results.push_back(r);
+  s->completed++;
+  delete j;
+}
+
+// One tick over the admitted jobs.  Returns a CUDA error to fail all jobs of the tick.
+cudaError_t tick(qcb_server* s, std::vector<Job*>& act, std::vector<int>& finishing_status) {
+  const int n = (int)act.size();
+  const uint32_t tile = (uint32_t)s->cfg.tile;
+  uint32_t nlevels = 0;
+  s->h_prefix[0] = 0;
+  std::vector<int> units(n, 0);
+  for (int k = 0; k < n; ++k) {
+    Job* j = act[k];
+    const qcb_lattice* L = j->spec.lat;
+    BatchLat& d = s->h_desc[k];
+    memset(&d, 0, sizeof d);
+    d.g = L->dev.g;
+    d.tile = tile;
+    if (j->ready) {
+      cudaError_t e = cudaStreamWaitEvent(s->stream, j->ready, 0);
+      if (e != cudaSuccess) return e;
+    }
+    if (j->spec.kind == QCB_JOB_SWEEPS) {
+      const int q = std::min(s->cfg.quantum_sweeps, j->spec.n_sweeps - j->done_units);
+      units[k] = q;
+      d.kind = BATCH_HB;
+      d.links = L->dev.links;
+      d.beta = j->spec.beta;
+      d.k0 = (uint32_t)j->spec.seed;
+      d.k1 = (uint32_t)(j->spec.seed >> 32);
+      d.sweep0 = (uint32_t)(j->spec.sweep_offset + (uint64_t)j->done_units);
+      d.ntiles = cdiv(d.g.Vh, tile);
+      d.nlev = 8u * (uint32_t)q;
+      d.n_hits = j->spec.n_hits;
+    } else {
+      if (!j->started) {
+        cudaError_t e = cudaMemcpyAsync(j->fw0, L->dev.links, L->bytes, cudaMemcpyDeviceToDevice, s->stream);
+        if (e != cudaSuccess) return e;
+        j->started = true;
+      }
+      const int q = std::min(s->cfg.quantum_steps, j->spec.n_steps - j->done_units);
+      units[k] = q;
+      d.kind = BATCH_FLOW;
+      const bool odd = (j->done_units & 1) != 0;
+      d.links = odd ? j->fw1 : j->fw0;
+      d.work = odd ? j->fw0 : j->fw1;
+      d.acc = j->acc;
+      d.ntiles = 8u * cdiv(d.g.Vh, tile);
+      d.nlev = 3u * (uint32_t)q;
+      d.eps = j->spec.eps;
+    }
+    if (d.nlev == 0) d.kind = BATCH_NONE;  // nothing to run this tick (measurement only)
+    if (d.nlev > nlevels) nlevels = d.nlev;
+    s->h_prefix[k + 1] = s->h_prefix[k] + d.ntiles;
+  }
+  cudaError_t e = cudaMemcpyAsync(s->d_desc, s->h_desc, n * sizeof(BatchLat), cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s->d_prefix, s->h_prefix, (n + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->d_done, 0, n * sizeof(uint32_t), s->stream);
+  if (e != cudaSuccess) return e;
+  if (nlevels > 0) {
+    BatchRun run;
+    run.lats = s->d_desc;
+    run.prefix = s->d_prefix;
+    run.nlat = n;
+    run.nlevels = nlevels;
+    run.per_level = s->h_prefix[n];
+    run.done = s->d_done;
+    run.status = s->d_status;
+    run.n_hits = 1;   // every descriptor carries its own n_hits / eps
+    run.eps = 0.02;
+    e = launch_batch(BATCH_MIXED, run, s->cfg.precision, s->cfg.storage, 128, 0, s->stream);
+    if (e != cudaSuccess) return e;
+  }
+  for (int k = 0; k < n; ++k) act[k]->done_units += units[k];
+  // Measurements of the finishing jobs: the plaquette of each finishing sweeps job and the
+  // clover (Q, E) of each finishing flow job's final buffer.  Result slots: finishing_status[k]
+  // = index into h_out (plaquette at [i], Q/E at [i], [i+1]); -1 for jobs that continue.
+  finishing_status.assign(n, -1);
+  std::vector<BatchLat> mh, mf;
+  std::vector<int> kh, kf;
+  for (int k = 0; k < n; ++k) {
+    Job* j = act[k];
+    const int total = (j->spec.kind == QCB_JOB_SWEEPS) ? j->spec.n_sweeps : j->spec.n_steps;
+    if (j->done_units < total && !j->cancel) continue;
+    BatchLat d = s->h_desc[k];
+    if (j->spec.kind == QCB_JOB_SWEEPS) {
+      mh.push_back(d);
+      kh.push_back(k);
+    } else {
+      d.links = (j->done_units & 1) ? j->fw1 : j->fw0;
+      mf.push_back(d);
+      kf.push_back(k);
+    }
+  }
+  const int m1 = (int)mh.size(), m2 = (int)mf.size();
+  if (m1 + m2 == 0) return cudaSuccess;
+  std::vector<BatchLat> md(mh);
+  md.insert(md.end(), mf.begin(), mf.end());
+  std::vector<uint32_t> rp(m1 + m2 + 2, 0);  // prefix of the sweeps list, then of the flow list
+  for (int a = 0; a < m1; ++a) rp[a + 1] = rp[a] + cdiv(mh[a].g.V, (uint32_t)batch_red_sites());
+  const uint32_t n1 = rp[m1];
+  uint32_t* rf = &rp[m1 + 1];
+  rf[0] = 0;
+  for (int a = 0; a < m2; ++a) rf[a + 1] = rf[a] + cdiv(mf[a].g.V, (uint32_t)batch_red_sites());
+  const uint32_t n2 = rf[m2];
+  const size_t need = 2 * (size_t)std::max(n1, n2);
+  if (need > s->scratch_cap) {
+    // grow the reduction scratch (outside the arena; rare)
+    cudaStreamSynchronize(s->stream);
+    cudaFree(s->d_scratch);
+    s->d_scratch = nullptr;
+    e = cudaMalloc(&s->d_scratch, need * sizeof(double));
+    if (e != cudaSuccess) return e;
+    s->scratch_cap = need;
+  }
+  // measurement descriptors and prefixes go after the tick's ones
+  BatchLat* dm = s->d_desc + s->cap;
+  uint32_t* dp = s->d_prefix + s->cap + 1;
+  e = cudaMemcpyAsync(dm, md.data(), md.size() * sizeof(BatchLat), cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dp, rp.data(), rp.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream);
+  if (e != cudaSuccess) return e;
+  // plaquettes -> d_out[0 .. m1), (Q, E) pairs -> d_out[m1 .. m1 + 2 m2)
+  if (m1)
+    e = launch_batch_plaquette(dm, dp, m1, n1, s->cfg.precision, s->cfg.storage, s->d_scratch, s->d_out, s->stream);
+  if (e == cudaSuccess && m2)
+    e = launch_batch_qe(dm + m1, dp + m1 + 1, m2, n2, s->cfg.precision, s->cfg.storage, s->d_scratch,
+                        s->d_out + m1, s->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s->h_out, s->d_out, (m1 + 2 * m2) * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+  for (int a = 0; a < m1; ++a) finishing_status[kh[a]] = a;
+  for (int a = 0; a < m2; ++a) finishing_status[kf[a]] = m1 + 2 * a;
+  // (the caller synchronises and distributes the results)
+  return e;
+}
+
+void scheduler(qcb_server* s) {
+  cudaSetDevice(s->ctx->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    // admit in arrival order while a slot and work space are available
+    while (!s->pending.empty() && (int)s->active.size() < s->cfg.max_jobs) {
+      Job* j = s->pending.front();
+      if (j->cancel) {
+        s->pending.pop_front();
+        finish(s, j, QCB_ERR_CANCELLED, 0, 0, 0, 0);
+        s->done_cv.notify_all();
+        continue;
+      }
+      if (j->spec.kind == QCB_JOB_FLOW) {
+        size_t off = 0;
+        const size_t need = ws_bytes_for(j->spec.lat);
+        if (!s->arena.alloc(need, &off)) break;  // head waits for space: FIFO, no overtaking
+        j->ws_off = off;
+        j->ws_bytes = need;
+        char* base = s->arena_base + off;
+        const size_t lb = (j->spec.lat->bytes + 255) & ~(size_t)255;
+        j->fw0 = base;
+        j->fw1 = base + lb;
+        j->acc = base + 2 * lb;
+      }
+      j->admit_s = s->now();
+      s->pending.pop_front();
+      s->active.push_back(j);
+      s->admitted++;
+    }
+    if ((int)s->active.size() > s->max_active) s->max_active = (int)s->active.size();
+    if (s->active.empty()) {
+      if (s->stop) break;
+      s->cv.wait_for(lk, std::chrono::milliseconds(50));
+      continue;
+    }
+    std::vector<Job*> act = s->active;
+    lk.unlock();
+    std::vector<int> fin_status;
+    cudaError_t e = tick(s, act, fin_status);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    int st = QCB_OK;
+    if (e == cudaSuccess) {
+      cudaMemcpy(s->h_status, s->d_status, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+      if (s->h_status[1] || s->h_status[2])
+        st = QCB_ERR_STATE;
+      else if (s->h_status[0])
+        st = QCB_ERR_KP_CAP;
+      if (s->h_status[0] || s->h_status[1] || s->h_status[2]) cudaMemset(s->d_status, 0, 4 * sizeof(uint32_t));
+    } else {
+      st = QCB_ERR_CUDA;
+      cudaGetLastError();
+    }
+    lk.lock();
+    s->ticks++;
+    // distribute results of the finishing jobs (or fail every job of a failed tick)
+    std::vector<Job*> keep;
+    for (size_t k = 0; k < act.size(); ++k) {
+      Job* j = act[k];
+      if (st != QCB_OK) {
+        finish(s, j, st, 0, 0, 0, 0);
+        continue;
+      }
+      const int slot = fin_status.empty() ? -1 : fin_status[k];
+      if (slot < 0) {
+        keep.push_back(j);
+        continue;
+      }
+      const int status = j->cancel ? QCB_ERR_CANCELLED : QCB_OK;
+      if (j->spec.kind == QCB_JOB_SWEEPS)
+        finish(s, j, status, s->h_out[slot], 0, 0, 0);
+      else
+        finish(s, j, status, 0, j->done_units * j->spec.eps, s->h_out[slot], s->h_out[slot + 1]);
+    }
+    s->active = keep;
+    s->done_cv.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int qcb_server_create(qcb_ctx* ctx, const qcb_server_config* cfg, qcb_server** out) {
+  if (!ctx || !cfg || !out) return set_error(QCB_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if ((cfg->precision != QCB_FP64 && cfg->precision != QCB_FP32) ||
+      (cfg->storage != QCB_R18 && cfg->storage != QCB_R12))
+    return set_error(QCB_ERR_INVALID, "bad precision or storage");
+  if (cfg->tile < 0 || (cfg->tile && ((cfg->tile & 31) || cfg->tile > 65536)))
+    return set_error(QCB_ERR_INVALID, "tile must be 0 or a multiple of 32 up to 65536");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_error(QCB_ERR_CUDA, "cudaSetDevice failed");
+  qcb_server* s = new (std::nothrow) qcb_server();
+  if (!s) return set_error(QCB_ERR_NOMEM, "host allocation failed");
+  s->ctx = ctx;
+  s->cfg = *cfg;
+  if (s->cfg.max_jobs <= 0) s->cfg.max_jobs = 256;
+  if (s->cfg.quantum_sweeps <= 0) s->cfg.quantum_sweeps = 2;
+  if (s->cfg.quantum_steps <= 0) s->cfg.quantum_steps = 4;
+  if (s->cfg.tile <= 0) s->cfg.tile = 256;
+  size_t budget = cfg->hbm_budget;
+  if (budget == 0) {
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    budget = (size_t)((double)fr * 0.8);
+  }
+  s->cap = s->cfg.max_jobs;
+  auto bail = [&](const char* what) {
+    cudaGetLastError();
+    cudaFree(s->arena_base);
+    cudaFree(s->d_desc);
+    cudaFreeHost(s->h_desc);
+    cudaFree(s->d_prefix);
+    cudaFreeHost(s->h_prefix);
+    cudaFree(s->d_done);
+    cudaFree(s->d_status);
+    cudaFreeHost(s->h_status);
+    cudaFree(s->d_out);
+    cudaFreeHost(s->h_out);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return set_error(QCB_ERR_NOMEM, what);
+  };
+  if (cudaMalloc(&s->arena_base, budget) != cudaSuccess) return bail("cannot allocate the server's work-space arena");
+  s->arena_bytes = budget;
+  s->arena.init(budget);
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&s->d_desc, 2 * (size_t)s->cap * sizeof(BatchLat)) != cudaSuccess ||
+      cudaMallocHost(&s->h_desc, (size_t)s->cap * sizeof(BatchLat)) != cudaSuccess ||
+      cudaMalloc(&s->d_prefix, (2 * (size_t)s->cap + 4) * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMallocHost(&s->h_prefix, (size_t)(s->cap + 1) * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&s->d_done, (size_t)s->cap * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&s->d_status, 4 * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMallocHost(&s->h_status, 4 * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&s->d_out, 3 * (size_t)s->cap * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&s->h_out, 3 * (size_t)s->cap * sizeof(double)) != cudaSuccess ||
+      cudaMemset(s->d_status, 0, 4 * sizeof(uint32_t)) != cudaSuccess)
+    return bail("cannot allocate server buffers");
+  s->t0 = std::chrono::steady_clock::now();
+  s->thr = std::thread(scheduler, s);
+  ctx_ref(ctx);
+  *out = s;
+  return QCB_OK;
+}
+
+int qcb_server_submit(qcb_server* s, const qcb_job* job, uint64_t* id) {
+  if (!s || !job || !job->lat) return set_error(QCB_ERR_INVALID, "null argument");
+  const qcb_lattice* L = job->lat;
+  if (L->ctx != s->ctx) return set_error(QCB_ERR_INVALID, "job lattice belongs to another context");
+  if (L->dev.prec != s->cfg.precision || L->dev.nr != s->cfg.storage)
+    return set_error(QCB_ERR_INVALID, "job lattice precision/storage differs from the server's");
+  if (job->kind == QCB_JOB_SWEEPS) {
+    if (job->n_sweeps < 0 || job->n_hits < 1 || !(job->beta > 0)) return set_error(QCB_ERR_INVALID, "bad sweeps job");
+  } else if (job->kind == QCB_JOB_FLOW) {
+    if (job->n_steps < 0) return set_error(QCB_ERR_INVALID, "bad flow job");
+    if (ws_bytes_for(L) > s->arena_bytes)
+      return set_error(QCB_ERR_NOMEM, "flow job needs more work space than the server's HBM budget");
+  } else {
+    return set_error(QCB_ERR_INVALID, "unknown job kind");
+  }
+  Job* j = new (std::nothrow) Job();
+  if (!j) return set_error(QCB_ERR_NOMEM, "host allocation failed");
+  j->spec = *job;
+  if (cudaEventCreateWithFlags(&j->ready, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventRecord(j->ready, s->ctx->stream) != cudaSuccess) {
+    cudaGetLastError();
+    delete j;
+    return set_error(QCB_ERR_CUDA, "cannot record the job's ready event");
+  }
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    j->id = s->next_id++;
+    j->submit_s = s->now();
+    s->pending.push_back(j);
+    s->submitted++;
+  }
+  s->cv.notify_all();
+  if (id) *id = j->id;
+  return QCB_OK;
+}
+
+int qcb_server_poll(qcb_server* s, qcb_job_result* out, int max, int* n) {
+  if (!s || !n || (max > 0 && !out)) return set_error(QCB_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  int k = 0;
+  while (k < max && !s->results.empty()) {
+    out[k++] = s->results.front();
+    s->results.pop_front();
+  }
+  *n = k;
+  return QCB_OK;
+}
+
+int qcb_server_drain(qcb_server* s, double timeout_s) {
+  if (!s) return set_error(QCB_ERR_INVALID, "null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  const bool ok = s->done_cv.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                                      [&] { return s->completed == s->submitted; });
+  return ok ? QCB_OK : set_error(QCB_ERR_STATE, "server drain timed out");
+}
+
+int qcb_server_cancel(qcb_server* s, uint64_t id) {
+  if (!s) return set_error(QCB_ERR_INVALID, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (Job* j : s->pending)
+    if (j->id == id) j->cancel = true;
+  for (Job* j : s->active)
+    if (j->id == id) j->cancel = true;
+  s->cv.notify_all();
+  return QCB_OK;
+}
+
+int qcb_server_stats_get(qcb_server* s, qcb_server_stats* st) {
+  if (!s || !st) return set_error(QCB_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  st->submitted = s->submitted;
+  st->admitted = s->admitted;
+  st->completed = s->completed;
+  st->ticks = s->ticks;
+  st->max_active = s->max_active;
+  st->arena_bytes = s->arena_bytes;
+  st->arena_peak = s->arena.peak();
+  return QCB_OK;
+}
+
+double qcb_server_clock(qcb_server* s) { return s ? s->now() : 0.0; }
+
+int qcb_server_destroy(qcb_server* s) {
+  if (!s) return QCB_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    for (Job* j : s->pending) j->cancel = true;
+    for (Job* j : s->active) j->cancel = true;
+  }
+  s->cv.notify_all();
+  if (s->thr.joinable()) s->thr.join();
+  for (Job* j : s->pending) {
+    if (j->ready) cudaEventDestroy(j->ready);
+    delete j;
+  }
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->stream);
+  cudaFree(s->arena_base);
+  cudaFree(s->d_desc);
+  cudaFreeHost(s->h_desc);
+  cudaFree(s->d_prefix);
+  cudaFreeHost(s->h_prefix);
+  cudaFree(s->d_done);
+  cudaFree(s->d_status);
+  cudaFreeHost(s->h_status);
+  cudaFree(s->d_scratch);
+  cudaFree(s->d_out);
+  cudaFreeHost(s->h_out);
+  cudaStreamDestroy(s->stream);
+  cudaGetLastError();
+  qcb_ctx* c = s->ctx;
+  delete s;
+  ctx_unref(c);
+  return QCB_OK;
+}
+
+}  // extern "C"

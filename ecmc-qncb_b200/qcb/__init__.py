@@ -26,13 +26,15 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import FP32, FP64, R12, R18, BatchPlan, HbParams, QcbError, check, lib
+from ._lib import (FP32, FP64, R12, R18, BatchPlan, HbParams, Job, JobResult, QcbError, ServerConfig, ServerStats,
+                   check, lib)
 
-__all__ = ["Context", "GaugeField", "Batch", "BatchPlan", "PhiloxStream", "GradientFlow", "HbParams", "QcbError", "heatbathcb",
+__all__ = ["Context", "GaugeField", "Batch", "BatchPlan", "Server", "PhiloxStream", "GradientFlow", "HbParams", "QcbError", "heatbathcb",
            "observables", "io", "save_ildg_clime", "read_ildg_clime", "FP32", "FP64", "R12", "R18",
            "device_count"]
 
@@ -51,6 +53,10 @@ class Context:
         check(lib().qcb_ctx_create(device, 0, C.byref(h)))
         self.h = h
         self.device = device
+        self._children = []  # weak references, in creation order
+
+    def _adopt(self, obj) -> None:
+        self._children.append(weakref.ref(obj))
 
     def sync(self) -> None:
         check(lib().qcb_ctx_sync(self.h))
@@ -70,7 +76,13 @@ class Context:
         return s.value or 0
 
     def close(self) -> None:
+        """Closes the objects created on this context (newest first), then the context."""
         if getattr(self, "h", None):
+            for ref in reversed(self._children):
+                obj = ref()
+                if obj is not None:
+                    obj.close()
+            self._children = []
             lib().qcb_ctx_destroy(self.h)
             self.h = None
 
@@ -103,6 +115,7 @@ class GaugeField:
         h = C.c_void_p()
         check(lib().qcb_lattice_create(ctx.h, (C.c_int * 4)(*dims), self.precision, self.storage, C.byref(h)))
         self.h = h
+        ctx._adopt(self)
 
     @property
     def volume(self) -> int:
@@ -184,6 +197,7 @@ class Batch:
         h = C.c_void_p()
         check(lib().qcb_batch_create(ctx.h, len(self.fields), arr, C.byref(h)))
         self.h = h
+        ctx._adopt(self)
 
     @property
     def n(self) -> int:
@@ -242,6 +256,67 @@ class Batch:
     def close(self) -> None:
         if getattr(self, "h", None):
             lib().qcb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+JOB_FLOW, JOB_SWEEPS = 1, 2
+
+
+class Server:
+    """Request server with continuous batching (qcb_server)."""
+
+    def __init__(self, ctx: Context, precision="fp32", storage: int = R12, hbm_budget: int = 0, max_jobs: int = 0,
+                 quantum_sweeps: int = 0, quantum_steps: int = 0, tile: int = 0):
+        cfg = ServerConfig(_precision(precision), int(storage), int(hbm_budget), int(max_jobs), int(quantum_sweeps),
+                           int(quantum_steps), int(tile))
+        h = C.c_void_p()
+        check(lib().qcb_server_create(ctx.h, C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.ctx = ctx
+        ctx._adopt(self)
+
+    def submit_sweeps(self, field: GaugeField, beta, n_sweeps, seed, sweep_offset=0, n_hits=1) -> int:
+        job = Job(JOB_SWEEPS, field.h.value, float(beta), int(seed), int(sweep_offset), int(n_sweeps), int(n_hits),
+                  0.0, 0)
+        jid = C.c_uint64()
+        check(lib().qcb_server_submit(self.h, C.byref(job), C.byref(jid)))
+        return jid.value
+
+    def submit_flow(self, field: GaugeField, eps, n_steps) -> int:
+        job = Job(JOB_FLOW, field.h.value, 0.0, 0, 0, 0, 1, float(eps), int(n_steps))
+        jid = C.c_uint64()
+        check(lib().qcb_server_submit(self.h, C.byref(job), C.byref(jid)))
+        return jid.value
+
+    def poll(self, max_results: int = 256):
+        buf = (JobResult * max_results)()
+        n = C.c_int()
+        check(lib().qcb_server_poll(self.h, buf, max_results, C.byref(n)))
+        return [buf[k] for k in range(n.value)]
+
+    def drain(self, timeout_s: float = 600.0) -> None:
+        check(lib().qcb_server_drain(self.h, float(timeout_s)))
+
+    def cancel(self, job_id: int) -> None:
+        check(lib().qcb_server_cancel(self.h, C.c_uint64(job_id)))
+
+    def clock(self) -> float:
+        return lib().qcb_server_clock(self.h)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        check(lib().qcb_server_stats_get(self.h, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().qcb_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

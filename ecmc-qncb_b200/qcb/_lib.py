@@ -31,6 +31,33 @@ class BatchPlan(C.Structure):
                 ("rk_per_group", C.c_int)]
 
 
+class Job(C.Structure):
+    """qcb_job."""
+    _fields_ = [("kind", C.c_int), ("lat", C.c_void_p), ("beta", C.c_double), ("seed", C.c_uint64),
+                ("sweep_offset", C.c_uint64), ("n_sweeps", C.c_int), ("n_hits", C.c_int), ("eps", C.c_double),
+                ("n_steps", C.c_int)]
+
+
+class JobResult(C.Structure):
+    """qcb_job_result."""
+    _fields_ = [("id", C.c_uint64), ("status", C.c_int), ("kind", C.c_int), ("plaquette", C.c_double),
+                ("t", C.c_double), ("q", C.c_double), ("e", C.c_double), ("submit_s", C.c_double),
+                ("admit_s", C.c_double), ("finish_s", C.c_double)]
+
+
+class ServerConfig(C.Structure):
+    """qcb_server_config."""
+    _fields_ = [("precision", C.c_int), ("storage", C.c_int), ("hbm_budget", C.c_size_t), ("max_jobs", C.c_int),
+                ("quantum_sweeps", C.c_int), ("quantum_steps", C.c_int), ("tile", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    """qcb_server_stats."""
+    _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("completed", C.c_uint64),
+                ("ticks", C.c_uint64), ("max_active", C.c_int), ("arena_bytes", C.c_size_t),
+                ("arena_peak", C.c_size_t)]
+
+
 class HbParams(C.Structure):
     """qcb_hb_params: RunParamsHbCB of the reference (src/io/params.h:46-63)."""
     _fields_ = [("L_core", C.c_int), ("n_core_dims", C.c_int), ("cold_start", C.c_int),
@@ -94,6 +121,14 @@ SIGNATURES = {
     "qcb_batch_run": (C.c_int, [_vp, C.POINTER(BatchPlan), _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _dp,
                                 _ip]),
     "qcb_batch_autotune": (C.c_int, [_vp, C.c_char_p]),
+    "qcb_server_create": (C.c_int, [_vp, C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
+    "qcb_server_submit": (C.c_int, [_vp, C.POINTER(Job), C.POINTER(C.c_uint64)]),
+    "qcb_server_poll": (C.c_int, [_vp, C.POINTER(JobResult), C.c_int, _ip]),
+    "qcb_server_drain": (C.c_int, [_vp, C.c_double]),
+    "qcb_server_cancel": (C.c_int, [_vp, C.c_uint64]),
+    "qcb_server_stats_get": (C.c_int, [_vp, C.POINTER(ServerStats)]),
+    "qcb_server_clock": (C.c_double, [_vp]),
+    "qcb_server_destroy": (C.c_int, [_vp]),
     "qcb_params_default": (C.c_int, [C.POINTER(HbParams)]),
     "qcb_params_load": (C.c_int, [C.c_char_p, C.POINTER(HbParams)]),
 }

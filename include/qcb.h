@@ -203,6 +203,64 @@ int qcb_batch_run(qcb_batch* b, const qcb_batch_plan* plan, const double* betas,
  * NULL = no cache) under keys "<device name>|<precision>-<storage>|<hb|flow>|LxLyLzLt". */
 int qcb_batch_autotune(qcb_batch* b, const char* cache_path);
 
+/* ---- serving ---------------------------------------------------------------------------
+ * No counterpart in the reference.  A request server with continuous batching: jobs
+ * (Wilson-flow measurements and generate-N-sweeps runs on resident lattices of any sizes)
+ * are admitted in arrival order while the server's device work-space arena (its HBM budget)
+ * and job slots allow; every tick advances every admitted job by a quantum of sweeps or RK3
+ * steps in ONE persistent launch (heatbath and flow items mixed), measures the jobs that
+ * finish, and admits new arrivals at the tick boundary.  A job's result does not depend on
+ * what else runs with it (counter-based random numbers, per-lattice arithmetic).  The
+ * server runs its own scheduler thread and CUDA stream on the context's device; a job's
+ * lattice is lent to the server from submission until its result is returned (a sweeps job
+ * updates it in place; a flow job flows a copy held in the server's arena). */
+typedef struct qcb_server qcb_server;
+enum { QCB_JOB_FLOW = 1, QCB_JOB_SWEEPS = 2 };
+typedef struct qcb_job {
+  int kind;               /* QCB_JOB_FLOW or QCB_JOB_SWEEPS */
+  qcb_lattice* lat;       /* resident input; precision and storage of the server */
+  double beta;            /* sweeps: coupling */
+  uint64_t seed;          /* sweeps: Philox key */
+  uint64_t sweep_offset;  /* sweeps: counter of the first sweep */
+  int n_sweeps, n_hits;   /* sweeps */
+  double eps;             /* flow: step size */
+  int n_steps;            /* flow: RK3 steps; Q and E are measured at t = n_steps * eps */
+} qcb_job;
+typedef struct qcb_job_result {
+  uint64_t id;
+  int status;            /* QCB_OK, QCB_ERR_CANCELLED, QCB_ERR_KP_CAP, ... */
+  int kind;
+  double plaquette;      /* sweeps: mean plaquette after the last sweep */
+  double t, q, e;        /* flow: flow time, clover charge, energy density */
+  double submit_s, admit_s, finish_s; /* server clock (s since creation) */
+} qcb_job_result;
+typedef struct qcb_server_config {
+  int precision, storage; /* of every job's lattice */
+  size_t hbm_budget;      /* bytes of device work space (0: 80% of the free memory) */
+  int max_jobs;           /* concurrent jobs (0: 256) */
+  int quantum_sweeps;     /* sweeps per sweeps-job per tick (0: 2) */
+  int quantum_steps;      /* RK3 steps per flow-job per tick (0: 4) */
+  int tile;               /* sites per work item (0: 256) */
+} qcb_server_config;
+typedef struct qcb_server_stats {
+  uint64_t submitted, admitted, completed, ticks;
+  int max_active;
+  size_t arena_bytes, arena_peak;
+} qcb_server_stats;
+int qcb_server_create(qcb_ctx* ctx, const qcb_server_config* cfg, qcb_server** out);
+/* Non-blocking; the job's lattice must not be touched until its result is polled. */
+int qcb_server_submit(qcb_server* s, const qcb_job* job, uint64_t* id);
+/* Non-blocking: copies up to max finished results (in completion order) into out. */
+int qcb_server_poll(qcb_server* s, qcb_job_result* out, int max, int* n);
+/* Blocks until every submitted job has finished or timeout_s elapses (QCB_ERR_STATE). */
+int qcb_server_drain(qcb_server* s, double timeout_s);
+/* A pending job is dropped, an admitted one stops at the next tick; its result carries
+ * QCB_ERR_CANCELLED. */
+int qcb_server_cancel(qcb_server* s, uint64_t id);
+int qcb_server_stats_get(qcb_server* s, qcb_server_stats* st);
+double qcb_server_clock(qcb_server* s);
+int qcb_server_destroy(qcb_server* s);
+
 /* ---- input file ----------------------------------------------------------------------
  * io::load_params(..., RunParamsHbCB&) (src/io/io.cpp:353-399) with the defaults of
  * src/io/params.h:46-63.  Host-only.  Strings are NUL-terminated and truncated to fit. */

@@ -239,3 +239,18 @@ def test_precision_fp32_flow_vs_fp64(ctx):
     r32 = qcb.observables.topo_charge_flowed(f32, gf, 6, 10).reshape(-1, 3)
     assert np.abs(r64[:, 1] - r32[:, 1]).max() < 1e-4
     assert np.abs(r64[:, 2] - r32[:, 2]).max() < 1e-4 * r64[:, 2].max()
+
+
+def test_context_destroyed_before_its_lattices():
+    """Destroying a context with live lattices defers the free until the last one goes."""
+    L = qcb._lib.lib()
+    c = qcb.Context(0)
+    f = qcb.GaugeField(c, (4, 4, 4, 4))
+    g = qcb.GaugeField(c, (4, 4, 4, 4))
+    raw_ctx, raw_f = c.h, f.h
+    c.h = None  # destroy through the C ABI directly, children still alive
+    assert L.qcb_ctx_destroy(raw_ctx) == 0
+    assert qcb.observables.mean_plaquette_global(f) == 1.0
+    f.h = None
+    assert L.qcb_lattice_destroy(raw_f) == 0
+    g.close()  # the last child frees the context
