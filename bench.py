@@ -33,6 +33,8 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "ecmc-qncb_b200"))
 
+from qcb import replicas  # noqa: E402  (host-side helpers only; the library loads lazily)
+
 L = 32
 BETA = 6.0
 SEED = 7
@@ -129,7 +131,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     lib = _lib.lib()
     dims = (L, L, L, L)
     V = L ** 4
-    seed = SEED + 1000 * rank  # independent replicas per rank
+    seed = replicas.replica_seed(SEED, rank)  # independent replicas per rank
 
     f32 = qcb.GaugeField(ctx, dims, "fp32", 12)
     gf = qcb.GradientFlow(FLOW_EPS)
@@ -152,11 +154,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, dist, device="cuda")
 
     for _ in range(args.warmup):
         step(f32)
@@ -234,25 +232,37 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                  "same_input": "FP64 heatbath output, flowed in FP32-12 and in FP64-18"}
 
     # ---- e2e through the C ABI with host buffers ------------------------------------------
+    # Heatbath e2e step: upload the FP64 links from a pinned host buffer (qcb_set_links),
+    # 500 sweeps, mean plaquette read back.  Flow e2e step: upload, flow to t = 4 with the
+    # (t, Q, E) records read back.
     host = torch.empty(V * 72, dtype=torch.float64).pin_memory()
     host.copy_(torch.from_numpy(f64.get_links().view(np.float64).reshape(-1)))
-    tqe_host = np.zeros(3 * FLOW_RECORDS)
-    e2e_ms = []
-    for k in range(args.warmup + args.steps):
-        barrier()
-        a, b = ev(), ev()
-        a.record(stream)
-        f32.set_links_ptr(host.data_ptr())
+
+    def e2e(body):
+        times = []
+        for k in range(args.warmup + args.steps):
+            barrier()
+            a, b = ev(), ev()
+            a.record(stream)
+            f32.set_links_ptr(host.data_ptr())
+            body()
+            b.record(stream)
+            b.synchronize()
+            if k >= args.warmup:
+                times.append(a.elapsed_time(b))
+        return max_over_ranks(statistics.mean(times))
+
+    plaq_box, tqe_box = [], []
+
+    def hb_body():
         _lib.check(lib.qcb_heatbath(f32.h, BETA, SWEEPS, 1, seed, 0))
-        tqe_host[:] = qcb.observables.topo_charge_flowed(f32, gf, FLOW_RECORDS, FLOW_RK)
-        plaq = qcb.observables.mean_plaquette_global(f32)
-        b.record(stream)
-        b.synchronize()
-        if k >= args.warmup:
-            e2e_ms.append(a.elapsed_time(b))
-    e2e_step_ms = max_over_ranks(statistics.mean(e2e_ms))
-    e2e_rate = world * SWEEPS * 4 * V / (e2e_step_ms / 1e3)
-    assert np.isfinite(plaq)
+        plaq_box.append(qcb.observables.mean_plaquette_global(f32))
+
+    e2e_hb_ms = e2e(hb_body)
+    e2e_fl_ms = e2e(lambda: tqe_box.append(qcb.observables.topo_charge_flowed(f32, gf, FLOW_RECORDS, FLOW_RK)))
+    e2e_rate = world * SWEEPS * 4 * V / (e2e_hb_ms / 1e3)
+    e2e_flow = world * FLOW_RECORDS * FLOW_RK * V / (e2e_fl_ms / 1e3)
+    assert np.isfinite(plaq_box[-1]) and np.all(np.isfinite(tqe_box[-1]))
 
     result = {
         "metric": METRIC, "value": hb_rate, "unit": "link-updates/s", "n_gpus": world, "steps": args.steps,
@@ -264,6 +274,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                    "flow_steps": FLOW_RECORDS * FLOW_RK, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (201 MB field vs 126 MB L2); no flush"},
         "flow": {"value": flow_rate, "unit": "site-steps/s", "ms_per_rk3": rk3_ms,
+                 "e2e": {"value": e2e_flow, "unit": "site-steps/s", "ms_per_step": e2e_fl_ms,
+                         "h2d_bytes_per_step": V * 72 * 8, "d2h_bytes_per_step": 3 * FLOW_RECORDS * 8},
                  "roofline": {"bound": "hbm", "achieved": flow_achieved, "peak": peak, "unit": "GB/s",
                               "frac": flow_achieved / peak, "peak_kind": peak_kind,
                               "traffic": traffic.get("flow_stage_fp32r12_per_rk3")}},
@@ -274,8 +286,9 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                      "unit": "GB/s", "frac": hb_achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic.get("hb_pass_fp32r12_per_launch"),
                      "algorithmic_bytes_per_launch": hb_bytes_launch, "launch_ms": hb_pass_ms},
-        "e2e": {"value": e2e_rate, "unit": "link-updates/s", "ms_per_step": e2e_step_ms,
-                "h2d_bytes_per_step": V * 72 * 8, "d2h_bytes_per_step": (3 * FLOW_RECORDS + 1) * 8},
+        "e2e": {"value": e2e_rate, "unit": "link-updates/s", "ms_per_step": e2e_hb_ms,
+                "h2d_bytes_per_step": V * 72 * 8, "d2h_bytes_per_step": 8,
+                "step": "qcb_set_links from pinned host FP64 links + 500 sweeps + plaquette to host"},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
@@ -444,6 +457,92 @@ def serving_section(ctx, n_requests=100, rate=20.0):
 
 
 # ---------------------------------------------------------------------------------------
+def large_workload(out_path=None) -> dict:
+    """Large single lattice: 64^4 (67M links) at beta = 6.3, Haar hot start from seed 99,
+    200 heatbath sweeps, then the flow to t = 6 (300 RK3 steps of 0.02) with Q/E every step,
+    in FP32 12-real storage (3.2 GB) and in FP64 18-real storage (9.7 GB).  The FP32 flow
+    runs on the FP64 heatbath output, so its Q/E errors against the FP64 flow are the
+    precision of the FP32 flow alone.  Per-kernel HBM GB/s are algorithmic bytes over
+    CUDA-event time per launch."""
+    import numpy as np
+    import torch
+
+    import qcb
+    from qcb import _lib
+
+    Lg, beta, seed, sweeps, n_flow, eps = 64, 6.3, 99, 200, 300, 0.02
+    dims, V = (Lg,) * 4, Lg ** 4
+    ctx = qcb.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    lib = _lib.lib()
+    gf = qcb.GradientFlow(eps)
+    peak, peak_kind = peaks()
+
+    def timed(fn, n=1):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(n):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / n
+
+    out = {"workload": "64^4 beta=6.3 hot start seed 99, 200 CM sweeps, flow to t=6 (300 RK3 eps=0.02, "
+                       "Q/E every step)", "lattice": list(dims), "kernels": {}}
+    res = {}
+    fields = {}
+    with Clocks(0) as clk:
+        for prec, nr in (("fp64", 18), ("fp32", 12)):
+            tag = f"{prec}-{nr}"
+            f = qcb.GaugeField(ctx, dims, prec, nr)
+            fields[tag] = f
+            f.hot_start(seed)
+            hb_ms = timed(lambda: _lib.check(lib.qcb_heatbath(f.h, beta, sweeps, 1, seed, 0)))
+            plaq = qcb.observables.mean_plaquette_global(f)
+            pass_ms = hb_ms / (8 * sweeps)
+            hb_gbs = HB_BYTES[(prec, nr)] * V / 2 / (pass_ms / 1e3) / 1e9
+            res[tag] = {"hb_total_s": hb_ms / 1e3, "hb_link_updates_per_s": sweeps * 4 * V / (hb_ms / 1e3),
+                        "plaquette_after_hb": plaq, "device_bytes": f.device_bytes}
+            out["kernels"][f"hb_pass {tag}"] = {"ms_per_launch": pass_ms, "GB/s": hb_gbs, "frac": hb_gbs / peak}
+        # the same configuration flowed in both storages
+        fields["fp32-12"].copy_from(fields["fp64-18"])
+        rec = {}
+        for tag, f in fields.items():
+            prec, nr = tag.split("-")
+            nr = int(nr)
+            scratch = qcb.GaugeField(ctx, dims, prec, nr)
+            scratch.copy_from(f)
+            rk3_ms = timed(lambda: _lib.check(lib.qcb_flow_steps(scratch.h, eps, 1)), 5)
+            qe_ms = timed(lambda: qcb.observables.topo_q_e_clover_global(scratch), 3)
+            scratch.close()
+            fl_gbs = FLOW_BYTES[(prec, nr)] * V / (rk3_ms / 1e3) / 1e9
+            out["kernels"][f"flow RK3 step {tag}"] = {"ms_per_step": rk3_ms, "GB/s": fl_gbs, "frac": fl_gbs / peak}
+            out["kernels"][f"clover Q/E {tag}"] = {"ms_per_measurement": qe_ms}
+            t_ms = timed(lambda: rec.__setitem__(tag, qcb.observables.topo_charge_flowed(f, gf, n_flow, 1)))
+            res[tag]["flow_total_s"] = t_ms / 1e3
+            res[tag]["flow_site_steps_per_s"] = n_flow * V / (t_ms / 1e3)
+            res[tag]["Q_t6"] = float(rec[tag][-2])
+            res[tag]["E_t6"] = float(rec[tag][-1])
+    r64, r32 = rec["fp64-18"].reshape(-1, 3), rec["fp32-12"].reshape(-1, 3)
+    out["results"] = res
+    out["precision"] = {"dQ_max": float(np.abs(r32[:, 1] - r64[:, 1]).max()),
+                        "dE_rel_max": float((np.abs(r32[:, 2] - r64[:, 2]) / np.abs(r64[:, 2])).max()),
+                        "same_input": "FP64 heatbath output, flowed in FP32-12 and in FP64-18"}
+    out["speedup_fp32_over_fp64"] = {
+        "hb": res["fp32-12"]["hb_link_updates_per_s"] / res["fp64-18"]["hb_link_updates_per_s"],
+        "flow_with_qe": res["fp32-12"]["flow_site_steps_per_s"] / res["fp64-18"]["flow_site_steps_per_s"]}
+    out["peak"] = {"hbm_gbs": peak, "kind": peak_kind}
+    out["clocks"] = clk.summary()
+    for f in fields.values():
+        f.close()
+    ctx.close()
+    if out_path:
+        Path(out_path).write_text(json.dumps(out, indent=1) + "\n")
+    return out
+
+
+# ---------------------------------------------------------------------------------------
 def _ref_worker(args):
     """One 'rank' of the reference schedule on a block of edge lb: sweeps then flow."""
     lb, sweeps, rk3, seed = args
@@ -493,13 +592,14 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="run only warmup + steps of the workload (for ncu); print launch counts")
     ap.add_argument("--storage", choices=["fp32-12", "fp64-18"], default="fp32-12")
+    ap.add_argument("--workload", choices=["precision", "large"], default="precision",
+                    help="large: the 64^4 single-lattice workload, printed as its own JSON object")
+    ap.add_argument("--out", default=None, help="also write the large-workload JSON to this path")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local_rank = replicas.env_rank()
 
     if args.impl == "reference":
         if rank != 0:
@@ -522,17 +622,11 @@ def main():
         print(json.dumps(out))
         return 0
 
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as tdist
-
-        torch.cuda.set_device(local_rank)
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                 device_id=torch.device("cuda", local_rank))
-        dist = tdist
+    if args.workload == "large":
+        if rank == 0:
+            print(json.dumps(large_workload(args.out)))
+        return 0
+    dist = replicas.init("nccl", timeout_s=300)
     if args.profile:
         return profile_steps(args)
     try:
