@@ -609,6 +609,49 @@ int qcb_heatbath(qcb_lattice* L, double beta, int n_sweeps, int n_hits, uint64_t
   return QCB_OK;
 }
 
+int qcb_heatbath_frozen(qcb_lattice* L, double beta, int n_sweeps, int n_hits, uint64_t seed, uint64_t sweep_offset,
+                        int l_core, const int shift[4]) {
+  CHECK_LAT(L);
+  if (n_sweeps < 0 || n_hits < 0) return fail(QCB_ERR_INVALID, "negative sweep or hit count");
+  if (!(beta > 0.0)) return fail(QCB_ERR_INVALID, "beta must be positive");
+  if (n_hits > (1 << 20)) return fail(QCB_ERR_INVALID, "too many hits");
+  if (!shift) return fail(QCB_ERR_INVALID, "null shift");
+  if (l_core < 1) return fail(QCB_ERR_INVALID, "l_core must be positive");
+  for (int d = 0; d < 4; ++d)
+    if (L->dev.g.L[d] % l_core != 0) return fail(QCB_ERR_INVALID, "l_core must divide every extent");
+  int fr[5] = {l_core, 0, 0, 0, 0};
+  for (int d = 0; d < 4; ++d) fr[1 + d] = ((shift[d] % l_core) + l_core) % l_core;
+  qcb_ctx* c = L->ctx;
+  LOCK(c);
+  TRY(set_device(c));
+  for (int s = 0; s < n_sweeps; ++s) {
+    const uint32_t sweep = (uint32_t)(sweep_offset + (uint64_t)s);
+    for (int mu = 0; mu < 4; ++mu)
+      for (int par = 0; par < 2; ++par) {
+        CU(launch_hb_pass(L->dev, mu, par, beta, seed, sweep, n_hits, c->d_status, c->stream, c->block, fr),
+           "heatbath pass");
+        c->launches++;
+      }
+  }
+  return QCB_OK;
+}
+
+int qcb_translate(qcb_lattice* L, const int shift[4]) {
+  CHECK_LAT(L);
+  if (!shift) return fail(QCB_ERR_INVALID, "null shift");
+  int sh[4];
+  for (int d = 0; d < 4; ++d) sh[d] = ((shift[d] % L->dev.g.L[d]) + L->dev.g.L[d]) % L->dev.g.L[d];
+  qcb_ctx* c = L->ctx;
+  LOCK(c);
+  TRY(set_device(c));
+  TRY(ensure_flow_space(L));
+  const LatDev tmp = with_links(L->dev, L->fw[0]);
+  CU(launch_translate(tmp, L->dev, sh, c->stream, 0), "translate");
+  c->launches++;
+  CU(cudaMemcpyAsync(L->dev.links, L->fw[0], L->bytes, cudaMemcpyDeviceToDevice, c->stream), "translate copy");
+  return QCB_OK;
+}
+
 // ---- observables ---------------------------------------------------------------------------
 int qcb_plaquette(qcb_lattice* L, double* out) {
   CHECK_LAT(L);

@@ -15,7 +15,16 @@
 // periodic indexing, updated by checkerboard sweeps (every link of a sweep is updated; no
 // frozen links, so no random translation is needed); the generator is Philox keyed by
 // `seed` with a sweep counter, and the seed file stores that pair.  Optional extra keys:
-// precision = fp64 | fp32 (default fp64), storage = 18 | 12 (default 18), device = N.
+// precision = fp64 | fp32 (default fp64), storage = 18 | 12 (default 18), device = N,
+// schedule = checkerboard | reference (default checkerboard).
+//
+// schedule = reference keeps the reference's update schedule on the one device: before each
+// shift's sweeps it draws the random shift (x, y, z, t), each uniform in [0, L_core), from
+// std::mt19937_64 (src/mpi/Shift.cpp:163-186) and prints it, and the sweeps leave the links
+// frozen by the L_core block faces of the shifted field unchanged
+// (src/geometry/GeometryCB.cpp:33-56).  The field is not moved each shift: the cumulative
+// shift is tracked and applied once (qcb_translate) before a configuration is written, so
+// the saved file is in the reference's frame.
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -26,6 +35,7 @@
 #include <iomanip>
 #include <iostream>
 #include <map>
+#include <random>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -221,10 +231,24 @@ struct Run {
   qcb_ctx* ctx = nullptr;
   qcb_lattice* lat = nullptr;
   uint64_t key = 0, sweep = 0;
+  bool ref_schedule = false;
+  int cum[4] = {0, 0, 0, 0};  // cumulative shift not yet applied to the stored links
+  std::mt19937_64 shift_rng;
 
+  // One shift of the run: N_samples * N_sweeps sweeps (heatbathcb::samples).
   void heatbath() {
     const int n = rp.N_samples * rp.N_sweeps;
-    CHECK(qcb_heatbath(lat, rp.beta, n, rp.N_hits, key, sweep), "heatbath");
+    if (ref_schedule) {
+      std::uniform_int_distribution<int> rand_l_shift(0, rp.L_core - 1);
+      int s[4];
+      for (int d = 0; d < 4; ++d) s[d] = rand_l_shift(shift_rng);
+      std::cout << "Shift (" << s[0] << ", " << s[1] << ", " << s[2] << ", " << s[3] << ")\n";
+      const int Lg = rp.L_core * rp.n_core_dims;
+      for (int d = 0; d < 4; ++d) cum[d] = (cum[d] + s[d]) % Lg;
+      CHECK(qcb_heatbath_frozen(lat, rp.beta, n, rp.N_hits, key, sweep, rp.L_core, cum), "heatbath");
+    } else {
+      CHECK(qcb_heatbath(lat, rp.beta, n, rp.N_hits, key, sweep), "heatbath");
+    }
     sweep += (uint64_t)n;
   }
   double plaquette() {
@@ -244,6 +268,10 @@ struct Run {
     return tqe;
   }
   void save_conf() {
+    if (cum[0] | cum[1] | cum[2] | cum[3]) {
+      CHECK(qcb_translate(lat, cum), "translate");
+      cum[0] = cum[1] = cum[2] = cum[3] = 0;
+    }
     fs::path dir = run_path(rp);
     ensure_dir(dir);
     fs::path p = dir / rp.run_name;
@@ -252,7 +280,7 @@ struct Run {
   }
 };
 
-void generate_hb_cb(Run& R, bool existing, int precision, int storage, int device) {
+void generate_hb_cb(Run& R, bool existing, int precision, int storage, int device, bool ref_schedule) {
   qcb_hb_params& rp = R.rp;
   const int L = rp.L_core * rp.n_core_dims;
   const int dims[4] = {L, L, L, L};
@@ -266,6 +294,8 @@ void generate_hb_cb(Run& R, bool existing, int precision, int storage, int devic
     CHECK(qcb_load_ildg(R.lat, p.string().c_str()), "read ILDG");
     load_seed(rp, &R.key, &R.sweep);
   }
+  R.ref_schedule = ref_schedule;
+  R.shift_rng.seed(R.key ^ R.sweep);
   save_params(rp);
   print_parameters(rp);
 
@@ -349,13 +379,22 @@ int main(int argc, char* argv[]) {
   if (ex.count("precision")) precision = (ex["precision"] == "fp32") ? QCB_FP32 : QCB_FP64;
   if (ex.count("storage")) storage = (ex["storage"] == "12") ? QCB_R12 : QCB_R18;
   if (ex.count("device")) device = atoi(ex["device"].c_str());
+  bool ref_schedule = false;
+  if (ex.count("schedule")) {
+    if (ex["schedule"] == "reference")
+      ref_schedule = true;
+    else if (ex["schedule"] != "checkerboard") {
+      std::cerr << "Error reading input : schedule must be checkerboard or reference" << std::endl;
+      return 1;
+    }
+  }
 
   fs::path config_file = run_path(R.rp) / R.rp.run_name;
   bool existing = fs::exists(config_file) && fs::exists(seed_path(R.rp));
   if (existing) std::cout << "All ranks found existing configuration. Resuming...\n";
 
   auto t0 = std::chrono::steady_clock::now();
-  generate_hb_cb(R, existing, precision, storage, device);
+  generate_hb_cb(R, existing, precision, storage, device, ref_schedule);
   double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   std::cout << "==========================================" << std::endl;
   std::cout << "Elapsed time : " << (long)total << "s\n";

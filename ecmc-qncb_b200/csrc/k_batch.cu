@@ -149,7 +149,7 @@ __device__ __forceinline__ void flow_item(const BatchRun& run, const BatchLat& B
 // first B.nlev levels only; its items at later levels are skipped (no wait, no release), and
 // a lattice of kind BATCH_NONE in a mixed launch takes part in none.
 template <typename S, int NR, int KINDS>
-__global__ void __launch_bounds__(128) k_batch(BatchRun run) {
+__global__ void __launch_bounds__(128, sizeof(S) == 4 ? 4 : 2) k_batch(BatchRun run) {
   const uint64_t total = (uint64_t)run.nlevels * run.per_level;
   uint32_t fails = 0;
   for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
@@ -209,7 +209,7 @@ cudaError_t launch_batch(int kind, const BatchRun& run, int prec, int nr, int bl
 // lattice is parity t >= Vh); partial sums parts[item] (and parts[nitems + item] for the
 // second quantity), then one warp per lattice adds its partials in a fixed order with
 // Neumaier compensation.
-constexpr int RED_SITES = 256;
+constexpr int RED_SITES = 128;
 int batch_red_sites() { return RED_SITES; }
 
 __device__ __forceinline__ double warp_sum_d(double v) {
@@ -238,7 +238,7 @@ __device__ __forceinline__ void block_sums(double* v, double* out) {
 }
 
 template <typename S, int NR, int WHAT>
-__global__ void __launch_bounds__(RED_SITES) k_batch_red(const BatchLat* __restrict__ lats,
+__global__ void __launch_bounds__(RED_SITES, sizeof(S) == 4 ? 4 : 2) k_batch_red(const BatchLat* __restrict__ lats,
                                                          const uint32_t* __restrict__ rprefix, int nlat,
                                                          uint32_t nitems, double* __restrict__ parts) {
   const uint32_t item = blockIdx.x;

@@ -25,44 +25,69 @@ struct HbMinBlocks {
   static constexpr int value = sizeof(S) == 4 ? 5 : 4;
 };
 
-template <typename S, int NR, int MU>
+// Frozen links of the reference's block decomposition (src/geometry/GeometryCB.cpp:33-56)
+// after a cumulative translation of the field by `shift`: link (x, mu) with
+// (x_d + shift_d) % lcore == 0 for some d != mu is not updated.  lcore == 0: none frozen.
+struct FrozenMask {
+  int lcore;
+  int shift[4];  // each in [0, lcore)
+};
+
+template <int MU>
+__device__ __forceinline__ bool is_frozen(const Coord& x, const FrozenMask& m) {
+#pragma unroll
+  for (int d = 0; d < 4; ++d)
+    if (d != MU && (x.c[d] + m.shift[d]) % m.lcore == 0) return true;
+  return false;
+}
+
+template <typename S, int NR, int MU, bool FROZEN>
 __global__ void __launch_bounds__(128, HbMinBlocks<S>::value) k_hb_pass(Geom g, Links<S, NR> f, int par, S beta, uint32_t k0,
-                                                 uint32_t k1, uint32_t sweep, int n_hits, uint32_t* status) {
+                                                 uint32_t k1, uint32_t sweep, int n_hits, uint32_t* status,
+                                                 FrozenMask fm) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.Vh) return;
+  if (FROZEN && is_frozen<MU>(cb_coord(g, par, i), fm)) return;
   const uint32_t fails = hb_update_link<Links<S, NR>, S, NR, MU>(g, f, par, i, beta, k0, k1, sweep, n_hits);
   if (fails) atomicAdd(status, fails);
 }
 
+template <typename S, int NR, int MU>
+static void hb_pass_launch(dim3 grid, int block, cudaStream_t s, const Geom& g, const Links<S, NR>& f, int par,
+                           S beta, uint32_t k0, uint32_t k1, uint32_t sweep, int n_hits, uint32_t* status,
+                           const FrozenMask& fm) {
+  if (fm.lcore > 0)
+    k_hb_pass<S, NR, MU, true><<<grid, block, 0, s>>>(g, f, par, beta, k0, k1, sweep, n_hits, status, fm);
+  else
+    k_hb_pass<S, NR, MU, false><<<grid, block, 0, s>>>(g, f, par, beta, k0, k1, sweep, n_hits, status, fm);
+}
+
 template <typename S, int NR>
 static cudaError_t hb_pass_impl(const LatDev& L, int mu, int par, double beta, uint64_t seed, uint32_t sweep,
-                                int n_hits, uint32_t* status, cudaStream_t s, int block) {
+                                int n_hits, uint32_t* status, cudaStream_t s, int block, FrozenMask fm) {
   Links<S, NR> f;
   f.p = reinterpret_cast<typename Links<S, NR>::V*>(L.links);
   f.stride = L.g.stride;
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
   dim3 grid(grid_for(L.g.Vh, block));
   switch (mu) {
-    case 0:
-      k_hb_pass<S, NR, 0><<<grid, block, 0, s>>>(L.g, f, par, S(beta), k0, k1, sweep, n_hits, status);
-      break;
-    case 1:
-      k_hb_pass<S, NR, 1><<<grid, block, 0, s>>>(L.g, f, par, S(beta), k0, k1, sweep, n_hits, status);
-      break;
-    case 2:
-      k_hb_pass<S, NR, 2><<<grid, block, 0, s>>>(L.g, f, par, S(beta), k0, k1, sweep, n_hits, status);
-      break;
-    default:
-      k_hb_pass<S, NR, 3><<<grid, block, 0, s>>>(L.g, f, par, S(beta), k0, k1, sweep, n_hits, status);
-      break;
+    case 0: hb_pass_launch<S, NR, 0>(grid, block, s, L.g, f, par, S(beta), k0, k1, sweep, n_hits, status, fm); break;
+    case 1: hb_pass_launch<S, NR, 1>(grid, block, s, L.g, f, par, S(beta), k0, k1, sweep, n_hits, status, fm); break;
+    case 2: hb_pass_launch<S, NR, 2>(grid, block, s, L.g, f, par, S(beta), k0, k1, sweep, n_hits, status, fm); break;
+    default: hb_pass_launch<S, NR, 3>(grid, block, s, L.g, f, par, S(beta), k0, k1, sweep, n_hits, status, fm); break;
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_hb_pass(const LatDev& L, int mu, int parity, double beta, uint64_t seed, uint32_t sweep,
-                           int n_hits, uint32_t* status, cudaStream_t s, int block) {
+                           int n_hits, uint32_t* status, cudaStream_t s, int block, const int* frozen) {
   if (block <= 0) block = 128;
-  QCB_DISPATCH_STORE(L, hb_pass_impl, L, mu, parity, beta, seed, sweep, n_hits, status, s, block);
+  FrozenMask fm = {0, {0, 0, 0, 0}};
+  if (frozen) {
+    fm.lcore = frozen[0];
+    for (int d = 0; d < 4; ++d) fm.shift[d] = frozen[1 + d];
+  }
+  QCB_DISPATCH_STORE(L, hb_pass_impl, L, mu, parity, beta, seed, sweep, n_hits, status, s, block, fm);
 }
 
 }  // namespace qcb

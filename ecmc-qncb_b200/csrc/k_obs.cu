@@ -15,8 +15,16 @@
 
 namespace qcb {
 
-constexpr int RED_THREADS = 256;
+constexpr int RED_THREADS = 128;
 constexpr int RED_BLOCKS = 148 * 8;
+
+// Minimum resident blocks per SM of the reduction kernels: the clover site evaluation is
+// the largest per-thread body; the bound keeps FP32 at 4 x 128 threads (128 registers) and
+// FP64 at 2 x 128 threads per SM.
+template <typename S>
+struct RedMinBlocks {
+  static constexpr int value = sizeof(S) == 4 ? 4 : 2;
+};
 
 int reduce_blocks() { return RED_BLOCKS; }
 
@@ -80,7 +88,7 @@ static int red_grid(const Geom& g) {
 }
 
 template <typename S, int NR>
-__global__ void __launch_bounds__(RED_THREADS) k_plaquette(Geom g, Links<S, NR> f, double* __restrict__ parts) {
+__global__ void __launch_bounds__(RED_THREADS, RedMinBlocks<S>::value) k_plaquette(Geom g, Links<S, NR> f, double* __restrict__ parts) {
   __shared__ double sh[RED_THREADS / 32];
   double acc = 0.0;
   const uint64_t n = (uint64_t)g.V;
@@ -129,7 +137,7 @@ cudaError_t launch_plaquette_partials(const LatDev& L, int nblocks, double* scra
 int reduce_threads() { return RED_THREADS; }
 
 template <typename S, int NR>
-__global__ void __launch_bounds__(RED_THREADS) k_clover_qe(Geom g, Links<S, NR> f, double* __restrict__ parts) {
+__global__ void __launch_bounds__(RED_THREADS, RedMinBlocks<S>::value) k_clover_qe(Geom g, Links<S, NR> f, double* __restrict__ parts) {
   typedef S R;
   __shared__ double sh[RED_THREADS / 32];
   double accq = 0.0, acce = 0.0;

@@ -15,6 +15,8 @@ Geom make_geom(const int dims[4]) {
   g.V = (uint32_t)dims[0] * (uint32_t)dims[1] * (uint32_t)dims[2] * (uint32_t)dims[3];
   g.Vh = g.V / 2;
   g.stride = (g.Vh + 63u) & ~63u;
+  const uint32_t dv[3] = {(uint32_t)g.Lxh, (uint32_t)dims[1], (uint32_t)dims[2]};
+  for (int k = 0; k < 3; ++k) g.rcp[k] = dv[k] == 1 ? 0xFFFFFFFFu : (uint32_t)((1ull << 32) / dv[k]);
   return g;
 }
 
@@ -295,6 +297,43 @@ static cudaError_t convert_dst(const LatDev& D, const LatDev& Sr, cudaStream_t s
 cudaError_t launch_convert(const LatDev& dst, const LatDev& src, cudaStream_t s, int block) {
   if (block <= 0) block = 256;
   QCB_DISPATCH_STORE(dst, convert_dst, dst, src, s, block);
+}
+
+// ---- translation ---------------------------------------------------------------------
+// dst(x) = src(x - sh) for every link: the reference's random shift of the whole field
+// (src/mpi/Shift.cpp:109-186) on one device.  sh[d] in [0, L_d).  Links are copied in the
+// storage type, bit for bit.
+template <typename S, int NR>
+__global__ void k_translate(Geom g, Links<S, NR> d, Links<S, NR> src, int4 sh) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.Vh) return;
+  const int mu = blockIdx.y >> 1, par = blockIdx.y & 1;
+  const Coord x = cb_coord(g, par, i);
+  const int shv[4] = {sh.x, sh.y, sh.z, sh.w};
+  uint32_t s = 0;
+  int ps = 0;
+#pragma unroll
+  for (int k = 3; k >= 0; --k) {
+    int y = x.c[k] - shv[k];
+    if (y < 0) y += g.L[k];
+    s = s * (uint32_t)g.L[k] + (uint32_t)y;
+    ps += y;
+  }
+  d.template store<S>(mu, par, i, src.template load<S>(mu, ps & 1, s >> 1));
+}
+template <typename S, int NR>
+static cudaError_t translate_impl(const LatDev& D, const LatDev& Sr, int4 sh, cudaStream_t s, int block) {
+  dim3 grid(grid_for(D.g.Vh, block), 8);
+  k_translate<S, NR><<<grid, block, 0, s>>>(D.g, links_of<S, NR>(D), links_of<S, NR>(Sr), sh);
+  return cudaGetLastError();
+}
+cudaError_t launch_translate(const LatDev& dst, const LatDev& src, const int shift[4], cudaStream_t s, int block) {
+  if (block <= 0) block = 256;
+  if (dst.prec != src.prec || dst.nr != src.nr || dst.links == src.links) return cudaErrorInvalidValue;
+  for (int d = 0; d < 4; ++d)
+    if (dst.g.L[d] != src.g.L[d] || shift[d] < 0 || shift[d] >= dst.g.L[d]) return cudaErrorInvalidValue;
+  const int4 sh = make_int4(shift[0], shift[1], shift[2], shift[3]);
+  QCB_DISPATCH_STORE(dst, translate_impl, dst, src, sh, s, block);
 }
 
 }  // namespace qcb

@@ -35,12 +35,15 @@ cudaError_t launch_aos_to_soa(const LatDev& L, const double* aos, uint32_t site0
 cudaError_t launch_soa_to_aos(const LatDev& L, double* aos, uint32_t site0, uint32_t nsites, int bswap,
                               cudaStream_t s, int block);
 cudaError_t launch_convert(const LatDev& dst, const LatDev& src, cudaStream_t s, int block);
+// dst(x) = src(x - shift), periodic (same geometry and storage; dst != src).
+cudaError_t launch_translate(const LatDev& dst, const LatDev& src, const int shift[4], cudaStream_t s, int block);
 
 // ---- heatbath (k_hb.cu) ------------------------------------------------------------
 // One checkerboard pass: every link (mu, parity) gets n_hits Cabibbo-Marinari hits.
-// status[0] counts KP draws that hit the attempt cap.
+// status[0] counts KP draws that hit the attempt cap.  frozen (optional) = {lcore, s0, s1,
+// s2, s3}: links with (x_d + s_d) % lcore == 0 for some d != mu are left unchanged.
 cudaError_t launch_hb_pass(const LatDev& L, int mu, int parity, double beta, uint64_t seed, uint32_t sweep,
-                           int n_hits, uint32_t* status, cudaStream_t s, int block);
+                           int n_hits, uint32_t* status, cudaStream_t s, int block, const int* frozen = nullptr);
 
 // ---- observables (k_obs.cu) --------------------------------------------------------
 // Reductions write per-block partial sums into scratch (nparts doubles per quantity,

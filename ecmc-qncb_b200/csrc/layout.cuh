@@ -30,7 +30,21 @@ struct Geom {
   uint32_t V;    // volume
   uint32_t Vh;   // V / 2
   uint32_t stride;  // allocation stride of one chunk array (>= Vh, multiple of 64)
+  uint32_t rcp[3];  // floor(2^32 / d) for d = Lxh, Ly, Lz (0xFFFFFFFF for d = 1)
 };
+
+// n / d and n % d by multiply-high with r = rcp of d: the estimate umulhi(n, r) is q or
+// q - 1 for every 32-bit n, so one correction step makes it exact.
+__device__ __forceinline__ uint32_t divmod_rcp(uint32_t n, uint32_t d, uint32_t r, uint32_t* rem) {
+  uint32_t q = __umulhi(n, r);
+  uint32_t m = n - q * d;
+  if (m >= d) {
+    ++q;
+    m -= d;
+  }
+  *rem = m;
+  return q;
+}
 
 struct Coord {
   int c[4];
@@ -40,12 +54,13 @@ struct Coord {
 // Coordinates of checkerboard site (parity p, index i).
 __device__ __forceinline__ Coord cb_coord(const Geom& g, int p, uint32_t i) {
   Coord r;
-  uint32_t q = i / (uint32_t)g.Lxh;
-  int xh = (int)(i - q * (uint32_t)g.Lxh);
-  uint32_t q2 = q / (uint32_t)g.L[1];
-  r.c[1] = (int)(q - q2 * (uint32_t)g.L[1]);
-  uint32_t q3 = q2 / (uint32_t)g.L[2];
-  r.c[2] = (int)(q2 - q3 * (uint32_t)g.L[2]);
+  uint32_t m;
+  const uint32_t q = divmod_rcp(i, (uint32_t)g.Lxh, g.rcp[0], &m);
+  const int xh = (int)m;
+  const uint32_t q2 = divmod_rcp(q, (uint32_t)g.L[1], g.rcp[1], &m);
+  r.c[1] = (int)m;
+  const uint32_t q3 = divmod_rcp(q2, (uint32_t)g.L[2], g.rcp[2], &m);
+  r.c[2] = (int)m;
   r.c[3] = (int)q3;
   r.c[0] = 2 * xh + ((p + r.c[1] + r.c[2] + r.c[3]) & 1);
   r.s = (uint32_t)r.c[0] + (uint32_t)g.L[0] * q;
@@ -121,6 +136,7 @@ template <typename S, int NR, int LM = LD_RO>
 struct Links {
   typedef typename Store<S, NR>::V V;
   static constexpr int NC = Store<S, NR>::NC;
+  static constexpr int NREAL = NR;
   V* p;
   uint32_t stride;
 
@@ -152,6 +168,31 @@ struct Links {
       }
     }
     if (NR == 12) reconstruct_row2(u);
+    return u;
+  }
+
+  // Rows 0 and 1 of link (mu, par, i) only; row 2 is left unset.  For 12-real storage this
+  // is the stored data with no reconstruction, for products whose row 2 is rebuilt after.
+  template <typename R>
+  __device__ __forceinline__ m3<R> load_rows01(int mu, int par, uint32_t i) const {
+    m3<R> u;
+    if constexpr (sizeof(V) == 4 * sizeof(S)) {
+      const V a = ldv<LM>(&p[idx(mu, par, 0, i)]);
+      const V b = ldv<LM>(&p[idx(mu, par, 1, i)]);
+      const V c = ldv<LM>(&p[idx(mu, par, 2, i)]);
+      u.e[0][0] = mk<R>(R(a.x), R(a.y));
+      u.e[0][1] = mk<R>(R(a.z), R(a.w));
+      u.e[0][2] = mk<R>(R(b.x), R(b.y));
+      u.e[1][0] = mk<R>(R(b.z), R(b.w));
+      u.e[1][1] = mk<R>(R(c.x), R(c.y));
+      u.e[1][2] = mk<R>(R(c.z), R(c.w));
+    } else {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const V v = ldv<LM>(&p[idx(mu, par, c, i)]);
+        u.e[c / 3][c % 3] = mk<R>(R(v.x), R(v.y));
+      }
+    }
     return u;
   }
 

@@ -34,8 +34,7 @@ __device__ __forceinline__ R site_plaquette(const Geom& g, const F& f, const Coo
 // Clover sum C_{mu nu}(x) of the four leaves, in the reference's leaf order
 // (observables_mpi.cpp:70-80).
 template <typename LF, typename R, int MU, int NU>
-__device__ __forceinline__ m3<R> clover_F(const Geom& g, const LF& f, const Coord& x, int par,
-                                          uint32_t i) {
+__device__ __forceinline__ m3<R> clover_C(const Geom& g, const LF& f, const Coord& x, int par, uint32_t i) {
   const int opp = par ^ 1;
   const uint32_t xpmu = cb_index(nb_full(g, x, MU, +1));            // opp
   const uint32_t xpnu = cb_index(nb_full(g, x, NU, +1));            // opp
@@ -73,44 +72,79 @@ __device__ __forceinline__ m3<R> clover_F(const Geom& g, const LF& f, const Coor
     m3<R> T2 = mul_na(f.template load<R>(NU, par, xpmumnu), Umu_x);
     acc_nn(C, T1, T2);
   }
-  // F = (C - C^dag) / 8
-  m3<R> Fm;
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int b = 0; b < 3; ++b)
-      Fm.e[a][b] = mk<R>(R(0.125) * (C.e[a][b].re - C.e[b][a].re), R(0.125) * (C.e[a][b].im + C.e[b][a].im));
-  return Fm;
+  return C;
 }
 
+// Anti-Hermitian 3x3 matrix in 9 reals: F_kk = i d[k], F_ij = o[.] for (i,j) = (0,1),
+// (0,2), (1,2), and F_ji = -conj(F_ij).
 template <typename R>
-__device__ __forceinline__ R sqnorm(const m3<R>& a) {
-  R s = 0;
+struct ah9 {
+  R d[3];
+  cx<R> o[3];
+};
+
+// F_{mu nu} = (C - C^dag) / 8 (observables_mpi.cpp:81-82) in compact form.
+template <typename R>
+__device__ __forceinline__ ah9<R> ah_from_clover(const m3<R>& C) {
+  ah9<R> F;
 #pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) s = fma(a.e[i][j].re, a.e[i][j].re, fma(a.e[i][j].im, a.e[i][j].im, s));
-  return s;
+  for (int k = 0; k < 3; ++k) F.d[k] = R(0.25) * C.e[k][k].im;
+  F.o[0] = mk<R>(R(0.125) * (C.e[0][1].re - C.e[1][0].re), R(0.125) * (C.e[0][1].im + C.e[1][0].im));
+  F.o[1] = mk<R>(R(0.125) * (C.e[0][2].re - C.e[2][0].re), R(0.125) * (C.e[0][2].im + C.e[2][0].im));
+  F.o[2] = mk<R>(R(0.125) * (C.e[1][2].re - C.e[2][1].re), R(0.125) * (C.e[1][2].im + C.e[2][1].im));
+  return F;
 }
 
-// q and e contributions of one pair of planes, sgn * Re tr(F_{M1 N1} F_{M2 N2}) and the two
-// squared norms.  Not inlined: each pair is a separate register allocation, which keeps
-// the six clover evaluations of a site from being interleaved into one block that spills.
-template <typename F, typename R, int M1, int N1, int M2, int N2>
-__device__ __noinline__ void pair_qe(Geom g, F f, Coord x, int par, uint32_t i, R sgn, R* q, R* e) {
-  const m3<R> Fa = clover_F<F, R, M1, N1>(g, f, x, par, i);
-  const m3<R> Fb = clover_F<F, R, M2, N2>(g, f, x, par, i);
-  *q += sgn * re_tr_nn(Fa, Fb);
-  *e += sqnorm(Fa) + sqnorm(Fb);
+// Re tr(A B) of two anti-Hermitian matrices: -sum_k a_k b_k - 2 sum_{i<j} Re(A_ij conj B_ij).
+template <typename R>
+__device__ __forceinline__ R re_tr_ah(const ah9<R>& A, const ah9<R>& B) {
+  R s = 0, t = 0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    s = fma(A.d[k], B.d[k], s);
+    t = fma(A.o[k].re, B.o[k].re, fma(A.o[k].im, B.o[k].im, t));
+  }
+  return -s - R(2) * t;
+}
+
+// |F|^2 = sum_ij |F_ij|^2 = sum_k d_k^2 + 2 sum_{i<j} |F_ij|^2.
+template <typename R>
+__device__ __forceinline__ R sqnorm_ah(const ah9<R>& A) {
+  R s = 0, t = 0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    s = fma(A.d[k], A.d[k], s);
+    t = fma(A.o[k].re, A.o[k].re, fma(A.o[k].im, A.o[k].im, t));
+  }
+  return s + R(2) * t;
+}
+
+// One clover plane.  Not inlined: each plane is its own register allocation (the 9-real
+// result crosses the call), which keeps the six planes of a site from being interleaved
+// into one block that spills.
+template <typename LF, typename R, int MU, int NU>
+__device__ __noinline__ void clover_plane(Geom g, LF f, Coord x, int par, uint32_t i, ah9<R>* out) {
+  *out = ah_from_clover(clover_C<LF, R, MU, NU>(g, f, x, par, i));
 }
 
 // Per-site unscaled clover sums: q_site = tr F01 F23 - tr F02 F13 + tr F03 F12 and
 // e_site = sum_{mu<nu} |F_mu nu|^2 (the 1/(4 pi^2) and 1/2 are applied to the totals).
 template <typename F, typename R>
 __device__ __forceinline__ void site_qe(const Geom& g, const F& f, const Coord& x, int par, uint32_t i, R* q, R* e) {
-  pair_qe<F, R, 0, 1, 2, 3>(g, f, x, par, i, R(1), q, e);
-  pair_qe<F, R, 0, 2, 1, 3>(g, f, x, par, i, R(-1), q, e);
-  pair_qe<F, R, 0, 3, 1, 2>(g, f, x, par, i, R(1), q, e);
+  ah9<R> a, b;
+  clover_plane<F, R, 0, 1>(g, f, x, par, i, &a);
+  clover_plane<F, R, 2, 3>(g, f, x, par, i, &b);
+  R qs = re_tr_ah(a, b), es = sqnorm_ah(a) + sqnorm_ah(b);
+  clover_plane<F, R, 0, 2>(g, f, x, par, i, &a);
+  clover_plane<F, R, 1, 3>(g, f, x, par, i, &b);
+  qs -= re_tr_ah(a, b);
+  es += sqnorm_ah(a) + sqnorm_ah(b);
+  clover_plane<F, R, 0, 3>(g, f, x, par, i, &a);
+  clover_plane<F, R, 1, 2>(g, f, x, par, i, &b);
+  qs += re_tr_ah(a, b);
+  es += sqnorm_ah(a) + sqnorm_ah(b);
+  *q += qs;
+  *e += es;
 }
 
 }  // namespace qcb

@@ -11,6 +11,53 @@
 
 namespace qcb {
 
+// The two staple terms of one plane (mu, nu), added to A.  Site indices: i = x (parity
+// par); ixmu = x+mu, ixnu = x+nu, ixmnu = x-nu (parity opp); ixmunu = x+mu-nu (parity par).
+// With 12-real storage each three-link product is an SU(3) matrix whose third row follows
+// from its first two, so only rows 0 and 1 of the first product are computed (from the
+// stored rows of the leading link, with no reconstruction of that link) and row 2 is
+// rebuilt once: forward T = U_nu(x+mu) U_mu(x+nu)^dag, A += T U_nu(x)^dag; backward
+// P = U_mu(x-nu) U_nu(x+mu-nu), A += P^dag U_nu(x-nu).
+template <typename F, typename R>
+__device__ __forceinline__ void staple_terms(m3<R>& A, const F& f, int nu, int mu, int par, int opp, uint32_t i,
+                                             uint32_t ixmu, uint32_t ixnu, uint32_t ixmunu, uint32_t ixmnu) {
+  if constexpr (F::NREAL == 12) {
+    {
+      const m3<R> U0 = f.template load_rows01<R>(nu, opp, ixmu);
+      const m3<R> U1 = f.template load<R>(mu, opp, ixnu);
+      m3<R> T = mul_na_rows01(U0, U1);
+      reconstruct_row2(T);
+      const m3<R> U2 = f.template load<R>(nu, par, i);
+      acc_na(A, T, U2);
+    }
+    {
+      const m3<R> V1 = f.template load_rows01<R>(mu, opp, ixmnu);
+      const m3<R> V0 = f.template load<R>(nu, par, ixmunu);
+      m3<R> P = mul_nn_rows01(V1, V0);
+      reconstruct_row2(P);
+      const m3<R> V2 = f.template load<R>(nu, opp, ixmnu);
+      acc_an(A, P, V2);
+    }
+  } else {
+    {
+      // forward: U_nu(x+mu) U_mu(x+nu)^dagger U_nu(x)^dagger
+      const m3<R> U0 = f.template load<R>(nu, opp, ixmu);
+      const m3<R> U1 = f.template load<R>(mu, opp, ixnu);
+      const m3<R> T = mul_na(U0, U1);
+      const m3<R> U2 = f.template load<R>(nu, par, i);
+      acc_na(A, T, U2);
+    }
+    {
+      // backward: U_nu(x+mu-nu)^dagger U_mu(x-nu)^dagger U_nu(x-nu)
+      const m3<R> V0 = f.template load<R>(nu, par, ixmunu);
+      const m3<R> V1 = f.template load<R>(mu, opp, ixmnu);
+      const m3<R> T = mul_aa(V0, V1);
+      const m3<R> V2 = f.template load<R>(nu, opp, ixmnu);
+      acc_nn(A, T, V2);
+    }
+  }
+}
+
 template <typename F, typename R, int MU>
 __device__ __forceinline__ m3<R> staple_sum(const Geom& g, const F& f, const Coord& x, int par, uint32_t i) {
   m3<R> A;
@@ -20,25 +67,10 @@ __device__ __forceinline__ m3<R> staple_sum(const Geom& g, const F& f, const Coo
 #pragma unroll
   for (int nu = 0; nu < 4; ++nu) {
     if (nu == MU) continue;
-    {
-      // forward: U_nu(x+mu) U_mu(x+nu)^dagger U_nu(x)^dagger
-      const uint32_t xnu = nb_full(g, x, nu, +1);
-      m3<R> U0 = f.template load<R>(nu, opp, cb_index(xmu));
-      m3<R> U1 = f.template load<R>(MU, opp, cb_index(xnu));
-      m3<R> T = mul_na(U0, U1);
-      m3<R> U2 = f.template load<R>(nu, par, i);
-      acc_na(A, T, U2);
-    }
-    {
-      // backward: U_nu(x+mu-nu)^dagger U_mu(x-nu)^dagger U_nu(x-nu)
-      const uint32_t xmunu = nb2_full(g, x, MU, +1, nu, -1);
-      const uint32_t xmnu = nb_full(g, x, nu, -1);
-      m3<R> V0 = f.template load<R>(nu, par, cb_index(xmunu));
-      m3<R> V1 = f.template load<R>(MU, opp, cb_index(xmnu));
-      m3<R> T = mul_aa(V0, V1);
-      m3<R> V2 = f.template load<R>(nu, opp, cb_index(xmnu));
-      acc_nn(A, T, V2);
-    }
+    const uint32_t xnu = nb_full(g, x, nu, +1);
+    const uint32_t xmunu = nb2_full(g, x, MU, +1, nu, -1);
+    const uint32_t xmnu = nb_full(g, x, nu, -1);
+    staple_terms<F, R>(A, f, nu, MU, par, opp, i, cb_index(xmu), cb_index(xnu), cb_index(xmunu), cb_index(xmnu));
   }
   return A;
 }
@@ -76,25 +108,10 @@ __device__ __forceinline__ m3<R> staple_sum_rt(const Geom& g, const F& f, const 
 #pragma unroll
   for (int nu = 0; nu < 4; ++nu) {
     if (nu == mu) continue;
-    {
-      // forward: U_nu(x+mu) U_mu(x+nu)^dagger U_nu(x)^dagger
-      const uint32_t xnu = (uint32_t)((int32_t)x.s + o.up[nu]);
-      m3<R> U0 = f.template load<R>(nu, opp, cb_index(xmu));
-      m3<R> U1 = f.template load<R>(mu, opp, cb_index(xnu));
-      m3<R> T = mul_na(U0, U1);
-      m3<R> U2 = f.template load<R>(nu, par, i);
-      acc_na(A, T, U2);
-    }
-    {
-      // backward: U_nu(x+mu-nu)^dagger U_mu(x-nu)^dagger U_nu(x-nu)
-      const uint32_t xmunu = (uint32_t)((int32_t)x.s + upmu + o.dn[nu]);
-      const uint32_t xmnu = (uint32_t)((int32_t)x.s + o.dn[nu]);
-      m3<R> V0 = f.template load<R>(nu, par, cb_index(xmunu));
-      m3<R> V1 = f.template load<R>(mu, opp, cb_index(xmnu));
-      m3<R> T = mul_aa(V0, V1);
-      m3<R> V2 = f.template load<R>(nu, opp, cb_index(xmnu));
-      acc_nn(A, T, V2);
-    }
+    const uint32_t xnu = (uint32_t)((int32_t)x.s + o.up[nu]);
+    const uint32_t xmunu = (uint32_t)((int32_t)x.s + upmu + o.dn[nu]);
+    const uint32_t xmnu = (uint32_t)((int32_t)x.s + o.dn[nu]);
+    staple_terms<F, R>(A, f, nu, mu, par, opp, i, cb_index(xmu), cb_index(xnu), cb_index(xmunu), cb_index(xmnu));
   }
   return A;
 }

@@ -181,6 +181,51 @@ __device__ __forceinline__ void acc_na(m3<R>& acc, const m3<R>& a, const m3<R>& 
       acc.e[i][j] = s;
     }
 }
+// acc += a^dagger * b
+template <typename R>
+__device__ __forceinline__ void acc_an(m3<R>& acc, const m3<R>& a, const m3<R>& b) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      cx<R> s = acc.e[i][j];
+      s = cfma_cn(a.e[0][i], b.e[0][j], s);
+      s = cfma_cn(a.e[1][i], b.e[1][j], s);
+      s = cfma_cn(a.e[2][i], b.e[2][j], s);
+      acc.e[i][j] = s;
+    }
+}
+// Rows 0 and 1 of a * b^dagger (only rows 0 and 1 of a are read; row 2 of c is unset).
+template <typename R>
+__device__ __forceinline__ m3<R> mul_na_rows01(const m3<R>& a, const m3<R>& b) {
+  m3<R> c;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      cx<R> s = mk<R>(0, 0);
+      s = cfma_nc(a.e[i][0], b.e[j][0], s);
+      s = cfma_nc(a.e[i][1], b.e[j][1], s);
+      s = cfma_nc(a.e[i][2], b.e[j][2], s);
+      c.e[i][j] = s;
+    }
+  return c;
+}
+// Rows 0 and 1 of a * b (only rows 0 and 1 of a are read; row 2 of c is unset).
+template <typename R>
+__device__ __forceinline__ m3<R> mul_nn_rows01(const m3<R>& a, const m3<R>& b) {
+  m3<R> c;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      cx<R> s = a.e[i][0] * b.e[0][j];
+      s = cfma(a.e[i][1], b.e[1][j], s);
+      s = cfma(a.e[i][2], b.e[2][j], s);
+      c.e[i][j] = s;
+    }
+  return c;
+}
 // Re tr(a * b)
 template <typename R>
 __device__ __forceinline__ R re_tr_nn(const m3<R>& a, const m3<R>& b) {

@@ -168,6 +168,16 @@ class GaugeField:
     def gauge_transform(self, seed: int) -> None:
         check(lib().qcb_gauge_transform(self.h, C.c_uint64(seed)))
 
+    def heatbath_frozen(self, beta, n_sweeps, n_hits, seed, sweep_offset, l_core, shift) -> None:
+        """Heatbath sweeps with the reference's frozen links of l_core blocks after the
+        cumulative translation `shift` (qcb_heatbath_frozen)."""
+        check(lib().qcb_heatbath_frozen(self.h, float(beta), int(n_sweeps), int(n_hits), C.c_uint64(seed),
+                                        C.c_uint64(sweep_offset), int(l_core), (C.c_int * 4)(*shift)))
+
+    def translate(self, shift) -> None:
+        """U'(x) = U(x - shift), periodic (mpi::shift::shift_field on one device)."""
+        check(lib().qcb_translate(self.h, (C.c_int * 4)(*shift)))
+
     def save_ildg(self, path) -> None:
         check(lib().qcb_save_ildg(self.h, os.fsencode(path)))
 

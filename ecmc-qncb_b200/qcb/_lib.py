@@ -105,6 +105,8 @@ SIGNATURES = {
     "qcb_load_ildg": (C.c_int, [_vp, C.c_char_p]),
     "qcb_ildg_probe": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "qcb_heatbath": (C.c_int, [_vp, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_uint64]),
+    "qcb_heatbath_frozen": (C.c_int, [_vp, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_uint64, C.c_int, _ip]),
+    "qcb_translate": (C.c_int, [_vp, _ip]),
     "qcb_plaquette": (C.c_int, [_vp, _dp]),
     "qcb_topo_qe": (C.c_int, [_vp, _dp, _dp]),
     "qcb_flow_measure": (C.c_int, [_vp, C.c_double, C.c_int, C.c_int, _dp]),

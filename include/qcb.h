@@ -125,6 +125,19 @@ int qcb_ildg_probe(const char* path, uint64_t* data_offset, uint64_t* data_bytes
  * reported by the next qcb_ctx_sync / result-returning call. */
 int qcb_heatbath(qcb_lattice* lat, double beta, int n_sweeps, int n_hits, uint64_t seed,
                  uint64_t sweep_offset);
+/* The same sweeps with the reference's frozen links (src/geometry/GeometryCB.cpp:33-56):
+ * the lattice is cut into blocks of edge l_core (one block per MPI rank in the reference)
+ * and, after the field has been translated by the cumulative shift `shift` of its random
+ * shifts (src/mpi/Shift.cpp:163-186), link (x, mu) is not updated when
+ * (x_d + shift_d) % l_core == 0 for some d != mu.  The lattice is not moved: the links keep
+ * the frame of the untranslated field, and qcb_translate by the cumulative shift gives the
+ * reference's frame.  l_core must divide every extent; shift is taken mod l_core. */
+int qcb_heatbath_frozen(qcb_lattice* lat, double beta, int n_sweeps, int n_hits, uint64_t seed,
+                        uint64_t sweep_offset, int l_core, const int shift[4]);
+/* Periodic translation of the whole field, U'(x) = U(x - shift) (mpi::shift::shift_field,
+ * src/mpi/Shift.cpp:109-160, on one device).  shift is taken mod the extents.  Uses the
+ * lattice's flow work space (allocated on first use). */
+int qcb_translate(qcb_lattice* lat, const int shift[4]);
 
 /* ---- observables -------------------------------------------------------------------
  * mpi::observables::mean_plaquette_global (src/observables/observables_mpi.cpp:8-43):

@@ -48,6 +48,10 @@ def lib():
         L.orc_mt19937_64_nth.restype = C.c_uint64
         L.orc_heatbath_cb.argtypes = [dp, ip, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_uint64]
         L.orc_heatbath_cb.restype = C.c_uint64
+        L.orc_heatbath_cb_frozen.argtypes = [dp, ip, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_uint64,
+                                             C.c_int, ip]
+        L.orc_heatbath_cb_frozen.restype = C.c_uint64
+        L.orc_shift_sequence.argtypes = [C.c_uint64, C.c_int, C.c_int, ip]
         L.orc_hot_start_philox.argtypes = [dp, ip, C.c_uint64]
         L.orc_gauge_transform_philox.argtypes = [dp, ip, C.c_uint64]
         L.orc_kp_samples.argtypes = [C.c_double, C.c_double, C.c_int, C.c_uint64, dp]
@@ -153,6 +157,22 @@ def heatbath_cb(u, dims, beta, n_sweeps, n_hits, seed, sweep_offset=0):
     fails = lib().orc_heatbath_cb(_dp(u), _dims(dims), beta, n_sweeps, n_hits, C.c_uint64(seed),
                                   C.c_uint64(sweep_offset))
     return u, int(fails)
+
+
+def heatbath_cb_frozen(u, dims, beta, n_sweeps, n_hits, seed, sweep_offset, lcore, shift):
+    """heatbath_cb with the reference's frozen links of lcore blocks after the cumulative
+    translation `shift` (links with (c_d + shift_d) % lcore == 0 for some d != mu stay)."""
+    u = np.array(u, np.complex128, copy=True)
+    fails = lib().orc_heatbath_cb_frozen(_dp(u), _dims(dims), beta, n_sweeps, n_hits, C.c_uint64(seed),
+                                         C.c_uint64(sweep_offset), int(lcore), (C.c_int * 4)(*shift))
+    return u, int(fails)
+
+
+def shift_sequence(seed: int, L: int, n: int) -> np.ndarray:
+    """The first n shift vectors (x, y, z, t) the reference draws from mt19937_64(seed)."""
+    out = (C.c_int * (4 * n))()
+    lib().orc_shift_sequence(C.c_uint64(seed), int(L), int(n), out)
+    return np.array(out[:], dtype=np.int64).reshape(n, 4)
 
 
 def gauge_transform_philox(u, dims, seed):

@@ -471,7 +471,21 @@ static bool cb_subgroup(M3& U, const M3& A, int i, int j, double beta, uint32_t 
   return true;
 }
 
-static uint64_t heatbath_cb(Lat& f, double beta, int n_sweeps, int n_hits, uint64_t seed, uint64_t sweep_offset) {
+// Frozen-link mask of the reference's block decomposition after a cumulative translation
+// `shift` of the field: the reference moves the field by s (new(c) = old(c - s)) and freezes
+// the links of local coordinate 0 in every direction d != mu of each L_core block
+// (src/geometry/GeometryCB.cpp:33-56).  In the frame of the untranslated field that is
+// link (c, mu) with (c_d + s_d) % lcore == 0 for some d != mu.
+static bool frozen_shifted(const int c[4], int mu, int lcore, const int* shift) {
+  for (int d = 0; d < 4; ++d)
+    if (d != mu && (c[d] + shift[d]) % lcore == 0) return true;
+  return false;
+}
+
+// Library schedule: checkerboard passes (mu, parity), Philox draws keyed by the link.  With
+// lcore > 0, the links frozen by frozen_shifted(., lcore, shift) are left unchanged.
+static uint64_t heatbath_cb(Lat& f, double beta, int n_sweeps, int n_hits, uint64_t seed, uint64_t sweep_offset,
+                            int lcore = 0, const int* shift = nullptr) {
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
   uint64_t fails = 0;
   for (int sw = 0; sw < n_sweeps; ++sw) {
@@ -482,6 +496,7 @@ static uint64_t heatbath_cb(Lat& f, double beta, int n_sweeps, int n_hits, uint6
           int c[4];
           f.coords(s, c);
           if (((c[0] + c[1] + c[2] + c[3]) & 1) != par) continue;
+          if (lcore > 0 && frozen_shifted(c, mu, lcore, shift)) continue;
           M3 A = staple(f, s, mu);
           M3 U = f.get(s, mu);
           const uint32_t link = (uint32_t)mu * (uint32_t)f.V + (uint32_t)s;
@@ -639,6 +654,24 @@ uint64_t orc_heatbath_cb(double* aos, const int dims[4], double beta, int n_swee
                          uint64_t sweep_offset) {
   Lat f = make(aos, dims);
   return heatbath_cb(f, beta, n_sweeps, n_hits, seed, sweep_offset);
+}
+
+// The same with the reference's frozen links of L_core blocks after a cumulative shift.
+uint64_t orc_heatbath_cb_frozen(double* aos, const int dims[4], double beta, int n_sweeps, int n_hits, uint64_t seed,
+                                uint64_t sweep_offset, int lcore, const int shift[4]) {
+  Lat f = make(aos, dims);
+  int sh[4];
+  for (int d = 0; d < 4; ++d) sh[d] = ((shift[d] % lcore) + lcore) % lcore;
+  return heatbath_cb(f, beta, n_sweeps, n_hits, seed, sweep_offset, lcore, sh);
+}
+
+// The first n shift vectors of mpi::shift::random_shift (src/mpi/Shift.cpp:163-172): four
+// draws of uniform_int_distribution<int>(0, L - 1) from std::mt19937_64(seed) per shift.
+int orc_shift_sequence(uint64_t seed, int L, int n, int* out) {
+  std::mt19937_64 rng(seed);
+  std::uniform_int_distribution<int> d(0, L - 1);
+  for (int k = 0; k < 4 * n; ++k) out[k] = d(rng);
+  return 0;
 }
 
 int orc_hot_start_philox(double* aos, const int dims[4], uint64_t seed) {

@@ -75,6 +75,21 @@ def test_plaquette_and_qe_fp64(ctx, dims):
     assert rel(e, eo) < 1e-12
 
 
+def test_smallest_extents(ctx):
+    """Extents of 2 (Lx/2 = 1: the coordinate division by one) and mixed sizes."""
+    dims = (2, 2, 4, 6)
+    u = orc.hot_philox(dims, 17)
+    f = lattice(ctx, u, dims)
+    assert rel(qcb.observables.mean_plaquette_global(f), orc.plaquette(u, dims)) < 1e-12
+    q, e = qcb.observables.topo_q_e_clover_global(f)
+    qo, eo = orc.topo_qe(u, dims)
+    assert abs(q - qo) < 1e-12 * max(1.0, abs(qo)) and rel(e, eo) < 1e-12
+    qcb._lib.check(qcb._lib.lib().qcb_heatbath(f.h, 6.0, 2, 1, 8, 0))
+    ref, fails = orc.heatbath_cb(u, dims, 6.0, 2, 1, 8, 0)
+    assert fails == 0
+    assert np.abs(f.get_links() - ref).max() < 1e-11
+
+
 @pytest.mark.parametrize("prec,nr,tol", [("fp64", 12, 1e-12), ("fp32", 18, 1e-6), ("fp32", 12, 1e-6)])
 def test_plaquette_and_qe_other_storage(ctx, prec, nr, tol):
     dims = (8, 8, 8, 8)

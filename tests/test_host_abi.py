@@ -170,3 +170,6 @@ def test_driver_rejects_bad_input(tmp_path):
     assert r.returncode == 1 and "Can't open file" in r.stderr
     r = subprocess.run([str(driver)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "Usage" in r.stderr
+    bad.write_text("L_core = 4\nschedule = lexicographic\n")
+    r = subprocess.run([str(driver), str(bad)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "schedule must be" in r.stderr
