@@ -503,7 +503,7 @@ def large_workload(out_path=None) -> dict:
             pass_ms = hb_ms / (8 * sweeps)
             hb_gbs = HB_BYTES[(prec, nr)] * V / 2 / (pass_ms / 1e3) / 1e9
             res[tag] = {"hb_total_s": hb_ms / 1e3, "hb_link_updates_per_s": sweeps * 4 * V / (hb_ms / 1e3),
-                        "plaquette_after_hb": plaq, "device_bytes": f.device_bytes}
+                        "plaquette_after_hb": plaq, "device_bytes": f.device_bytes()}
             out["kernels"][f"hb_pass {tag}"] = {"ms_per_launch": pass_ms, "GB/s": hb_gbs, "frac": hb_gbs / peak}
         # the same configuration flowed in both storages
         fields["fp32-12"].copy_from(fields["fp64-18"])

@@ -7,6 +7,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#ifndef QCB_PACKED_FP32
+#define QCB_PACKED_FP32 0
+#endif
+
 namespace qcb {
 
 template <typename R>
@@ -69,6 +73,36 @@ __device__ __forceinline__ cx<R> cfma_cc(cx<R> a, cx<R> b, cx<R> acc) {
   acc.im = fma(-a.im, b.re, acc.im);
   return acc;
 }
+
+#if QCB_PACKED_FP32
+// FP32 complex multiply-adds as two packed FP32 FMAs (__ffma2_rn, sm_100): lane 0 carries the
+// real part, lane 1 the imaginary part.  Each lane performs the same two fused operations in
+// the same order as the scalar forms above, so the results are bit-identical to them.
+template <>
+__device__ __forceinline__ cx<float> cfma(cx<float> a, cx<float> b, cx<float> acc) {
+  float2 r = __ffma2_rn(make_float2(a.re, a.re), make_float2(b.re, b.im), make_float2(acc.re, acc.im));
+  r = __ffma2_rn(make_float2(-a.im, a.im), make_float2(b.im, b.re), r);
+  return mk(r.x, r.y);
+}
+template <>
+__device__ __forceinline__ cx<float> cfma_cn(cx<float> a, cx<float> b, cx<float> acc) {
+  float2 r = __ffma2_rn(make_float2(a.re, a.re), make_float2(b.re, b.im), make_float2(acc.re, acc.im));
+  r = __ffma2_rn(make_float2(a.im, -a.im), make_float2(b.im, b.re), r);
+  return mk(r.x, r.y);
+}
+template <>
+__device__ __forceinline__ cx<float> cfma_nc(cx<float> a, cx<float> b, cx<float> acc) {
+  float2 r = __ffma2_rn(make_float2(a.re, -a.re), make_float2(b.re, b.im), make_float2(acc.re, acc.im));
+  r = __ffma2_rn(make_float2(a.im, a.im), make_float2(b.im, b.re), r);
+  return mk(r.x, r.y);
+}
+template <>
+__device__ __forceinline__ cx<float> cfma_cc(cx<float> a, cx<float> b, cx<float> acc) {
+  float2 r = __ffma2_rn(make_float2(a.re, -a.re), make_float2(b.re, b.im), make_float2(acc.re, acc.im));
+  r = __ffma2_rn(make_float2(-a.im, -a.im), make_float2(b.im, b.re), r);
+  return mk(r.x, r.y);
+}
+#endif
 
 template <typename R>
 struct m3 {
