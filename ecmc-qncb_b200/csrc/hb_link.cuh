@@ -39,28 +39,14 @@ struct KpMath<float> {
   }
 };
 
-// One SU(2) subgroup update of U for subgroup (a, b), block entries of W = U A.
-template <typename R, int A_, int B_>
-__device__ __forceinline__ bool cm_subgroup(m3<R>& U, const m3<R>& A, R beta, uint32_t link, uint32_t sweep,
-                                            uint32_t hsg, uint32_t k0, uint32_t k1) {
-  // W_ij = sum_k U_ik A_kj for the four block entries.
-  cx<R> Waa = mk<R>(0, 0), Wab = mk<R>(0, 0), Wba = mk<R>(0, 0), Wbb = mk<R>(0, 0);
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    Waa = cfma(U.e[A_][k], A.e[k][A_], Waa);
-    Wab = cfma(U.e[A_][k], A.e[k][B_], Wab);
-    Wba = cfma(U.e[B_][k], A.e[k][A_], Wba);
-    Wbb = cfma(U.e[B_][k], A.e[k][B_], Wbb);
-  }
-  // Quaternion of [[Waa, Wab], [Wba, Wbb]].
-  R w0 = (Waa.re + Wbb.re) * R(0.5);
-  R w1 = (Wab.im + Wba.im) * R(0.5);
-  R w2 = (Wab.re - Wba.re) * R(0.5);
-  R w3 = (Waa.im - Wbb.im) * R(0.5);
-  R kk = sqrt(w0 * w0 + w1 * w1 + w2 * w2 + w3 * w3);
-  R ik = R(1) / kk;
-  R v0 = w0 * ik, v1 = w1 * ik, v2 = w2 * ik, v3 = w3 * ik;
-  R alpha = beta * kk * R(2.0) / R(3.0);
+// The SU(2) draw of one subgroup update: a0 from the Kennedy-Pendleton density
+// sqrt(1-a0^2) exp(alpha a0), then (a1, a2, a3) uniform on the sphere of radius
+// sqrt(1-a0^2).  Returns false when the KP attempts hit the cap.  FP64 calls one
+// out-of-line copy for the three subgroups (measured 4% faster per pass on 32^4, the
+// smaller code); FP32 inlines it (no difference measured).
+template <typename R>
+__device__ __forceinline__ bool kp_draw_inline(R alpha, uint32_t link, uint32_t sweep, uint32_t hsg, uint32_t k0,
+                                               uint32_t k1, R* x) {
   R mhalf_over_alpha = R(-0.5) / alpha;
   // Kennedy-Pendleton draw of a0 with density sqrt(1-a0^2) exp(alpha a0).
   R a0 = 0;
@@ -98,7 +84,51 @@ __device__ __forceinline__ bool cm_subgroup(m3<R>& U, const m3<R>& A, R beta, ui
   R rs = sqrt(fmax(R(0), R(1) - a0 * a0));
   R sphi, cphi;
   KpMath<R>::sincos2pi(uphi, &sphi, &cphi);
-  R x0 = a0, x1 = rs * sth * cphi, x2 = rs * sth * sphi, x3 = rs * cth;
+  x[0] = a0;
+  x[1] = rs * sth * cphi;
+  x[2] = rs * sth * sphi;
+  x[3] = rs * cth;
+  return true;
+}
+
+template <typename R>
+__device__ __noinline__ bool kp_draw(R alpha, uint32_t link, uint32_t sweep, uint32_t hsg, uint32_t k0, uint32_t k1,
+                                     R* x) {
+  return kp_draw_inline<R>(alpha, link, sweep, hsg, k0, k1, x);
+}
+
+// One SU(2) subgroup update of U for subgroup (a, b), block entries of W = U A.
+template <typename R, int A_, int B_>
+__device__ __forceinline__ bool cm_subgroup(m3<R>& U, const m3<R>& A, R beta, uint32_t link, uint32_t sweep,
+                                            uint32_t hsg, uint32_t k0, uint32_t k1) {
+  // W_ij = sum_k U_ik A_kj for the four block entries.
+  cx<R> Waa = mk<R>(0, 0), Wab = mk<R>(0, 0), Wba = mk<R>(0, 0), Wbb = mk<R>(0, 0);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    Waa = cfma(U.e[A_][k], A.e[k][A_], Waa);
+    Wab = cfma(U.e[A_][k], A.e[k][B_], Wab);
+    Wba = cfma(U.e[B_][k], A.e[k][A_], Wba);
+    Wbb = cfma(U.e[B_][k], A.e[k][B_], Wbb);
+  }
+  // Quaternion of [[Waa, Wab], [Wba, Wbb]].
+  R w0 = (Waa.re + Wbb.re) * R(0.5);
+  R w1 = (Wab.im + Wba.im) * R(0.5);
+  R w2 = (Wab.re - Wba.re) * R(0.5);
+  R w3 = (Waa.im - Wbb.im) * R(0.5);
+  R kk = sqrt(w0 * w0 + w1 * w1 + w2 * w2 + w3 * w3);
+  R ik = R(1) / kk;
+  R v0 = w0 * ik, v1 = w1 * ik, v2 = w2 * ik, v3 = w3 * ik;
+  R alpha = beta * kk * R(2.0) / R(3.0);
+  R x0, x1, x2, x3;
+  if constexpr (sizeof(R) == 8) {
+    R xq[4];
+    if (!kp_draw<R>(alpha, link, sweep, hsg, k0, k1, xq)) return false;
+    x0 = xq[0], x1 = xq[1], x2 = xq[2], x3 = xq[3];
+  } else {
+    R xq[4];
+    if (!kp_draw_inline<R>(alpha, link, sweep, hsg, k0, k1, xq)) return false;
+    x0 = xq[0], x1 = xq[1], x2 = xq[2], x3 = xq[3];
+  }
   // r = x * adj(v), adj(v) = (v0, -v1, -v2, -v3).
   R q0 = x0 * v0 + x1 * v1 + x2 * v2 + x3 * v3;
   R q1 = -x0 * v1 + x1 * v0 - x2 * v3 + x3 * v2;

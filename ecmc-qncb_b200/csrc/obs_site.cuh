@@ -4,7 +4,7 @@
 // References: mean_plaquette_local (src/observables/observables_mpi.cpp:8-29),
 // clover_site and local_q_e_clover (observables_mpi.cpp:61-107).
 #pragma once
-#include "layout.cuh"
+#include "staple.cuh"
 
 namespace qcb {
 
@@ -31,50 +31,6 @@ __device__ __forceinline__ R site_plaquette(const Geom& g, const F& f, const Coo
 }
 
 // ---- clover Q and E -------------------------------------------------------------------
-// Clover sum C_{mu nu}(x) of the four leaves, in the reference's leaf order
-// (observables_mpi.cpp:70-80).
-template <typename LF, typename R, int MU, int NU>
-__device__ __forceinline__ m3<R> clover_C(const Geom& g, const LF& f, const Coord& x, int par, uint32_t i) {
-  const int opp = par ^ 1;
-  const uint32_t xpmu = cb_index(nb_full(g, x, MU, +1));            // opp
-  const uint32_t xpnu = cb_index(nb_full(g, x, NU, +1));            // opp
-  const uint32_t xmmu = cb_index(nb_full(g, x, MU, -1));            // opp
-  const uint32_t xmnu = cb_index(nb_full(g, x, NU, -1));            // opp
-  const uint32_t xmmupnu = cb_index(nb2_full(g, x, MU, -1, NU, +1));  // par
-  const uint32_t xmmumnu = cb_index(nb2_full(g, x, MU, -1, NU, -1));  // par
-  const uint32_t xpmumnu = cb_index(nb2_full(g, x, MU, +1, NU, -1));  // par
-  const m3<R> Umu_x = f.template load<R>(MU, par, i);
-  const m3<R> Unu_x = f.template load<R>(NU, par, i);
-  m3<R> C;
-  {
-    // U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
-    m3<R> T1 = mul_nn(Umu_x, f.template load<R>(NU, opp, xpmu));
-    m3<R> T2 = mul_nn(Unu_x, f.template load<R>(MU, opp, xpnu));
-    C = mul_na(T1, T2);
-  }
-  const m3<R> Umu_xmmu = f.template load<R>(MU, opp, xmmu);
-  {
-    // U_nu(x) U_mu(x-mu+nu)^dag U_nu(x-mu)^dag U_mu(x-mu)
-    m3<R> T1 = mul_na(Unu_x, f.template load<R>(MU, par, xmmupnu));
-    m3<R> T2 = mul_an(f.template load<R>(NU, opp, xmmu), Umu_xmmu);
-    acc_nn(C, T1, T2);
-  }
-  const m3<R> Unu_xmnu = f.template load<R>(NU, opp, xmnu);
-  {
-    // U_mu(x-mu)^dag U_nu(x-mu-nu)^dag U_mu(x-mu-nu) U_nu(x-nu)
-    m3<R> T1 = mul_aa(Umu_xmmu, f.template load<R>(NU, par, xmmumnu));
-    m3<R> T2 = mul_nn(f.template load<R>(MU, par, xmmumnu), Unu_xmnu);
-    acc_nn(C, T1, T2);
-  }
-  {
-    // U_nu(x-nu)^dag U_mu(x-nu) U_nu(x+mu-nu) U_mu(x)^dag
-    m3<R> T1 = mul_an(Unu_xmnu, f.template load<R>(MU, opp, xmnu));
-    m3<R> T2 = mul_na(f.template load<R>(NU, par, xpmumnu), Umu_x);
-    acc_nn(C, T1, T2);
-  }
-  return C;
-}
-
 // Anti-Hermitian 3x3 matrix in 9 reals: F_kk = i d[k], F_ij = o[.] for (i,j) = (0,1),
 // (0,2), (1,2), and F_ji = -conj(F_ij).
 template <typename R>
@@ -119,30 +75,104 @@ __device__ __forceinline__ R sqnorm_ah(const ah9<R>& A) {
   return s + R(2) * t;
 }
 
-// One clover plane.  Not inlined: each plane is its own register allocation (the 9-real
-// result crosses the call), which keeps the six planes of a site from being interleaved
-// into one block that spills.
-template <typename LF, typename R, int MU, int NU>
-__device__ __noinline__ void clover_plane(Geom g, LF f, Coord x, int par, uint32_t i, ah9<R>* out) {
-  *out = ah_from_clover(clover_C<LF, R, MU, NU>(g, f, x, par, i));
+// Product helpers for the clover leaves.  With 12-real storage a product of two SU(3)
+// matrices is formed from the stored rows 0 and 1 of its first factor (no reconstruction of
+// that link) and its row 2 is rebuilt by the cross product; with 18-real storage the full
+// product is formed.
+template <typename LF, typename R>
+__device__ __forceinline__ m3<R> lead(const LF& f, int mu, int par, uint32_t i) {
+  if constexpr (LF::NREAL == 12) return f.template load_rows01<R>(mu, par, i);
+  else return f.template load<R>(mu, par, i);
+}
+template <typename LF, typename R>
+__device__ __forceinline__ m3<R> prod_nn(const m3<R>& a, const m3<R>& b) {
+  if constexpr (LF::NREAL == 12) {
+    m3<R> c = mul_nn_rows01(a, b);
+    reconstruct_row2(c);
+    return c;
+  } else {
+    return mul_nn(a, b);
+  }
+}
+template <typename LF, typename R>
+__device__ __forceinline__ m3<R> prod_na(const m3<R>& a, const m3<R>& b) {
+  if constexpr (LF::NREAL == 12) {
+    m3<R> c = mul_na_rows01(a, b);
+    reconstruct_row2(c);
+    return c;
+  } else {
+    return mul_na(a, b);
+  }
+}
+
+// Clover plane (mu, nu) at site x with the plane chosen at run time, so that the six planes
+// of a site run through one copy of this code (one body in the instruction cache).  The four
+// leaves, in the reference's order (observables_mpi.cpp:70-80), each grouped as products of
+// SU(3) matrices whose first factor is a stored link:
+//   L1 = [U_mu(x) U_nu(x+mu)] [U_nu(x) U_mu(x+nu)]^dag
+//   L2 = U_nu(x) [U_nu(x-mu) U_mu(x-mu+nu)]^dag U_mu(x-mu)
+//   L3 = [U_nu(x-mu-nu) U_mu(x-mu)]^dag [U_mu(x-mu-nu) U_nu(x-nu)]
+//   L4 = U_nu(x-nu)^dag [U_mu(x-nu) U_nu(x+mu-nu)] U_mu(x)^dag
+// xs is the full index of x; o its neighbour offsets.
+template <typename LF, typename R>
+__device__ __noinline__ void clover_plane_rt(LF f, uint32_t xs, NbOff o, int mu, int nu, int par, uint32_t i,
+                                             ah9<R>* out) {
+  const int opp = par ^ 1;
+  const int32_t upmu = sel4(o.up, mu), upnu = sel4(o.up, nu), dnmu = sel4(o.dn, mu), dnnu = sel4(o.dn, nu);
+  const int32_t s = (int32_t)xs;
+  const uint32_t xpmu = (uint32_t)(s + upmu) >> 1, xpnu = (uint32_t)(s + upnu) >> 1;       // opp
+  const uint32_t xmmu = (uint32_t)(s + dnmu) >> 1, xmnu = (uint32_t)(s + dnnu) >> 1;       // opp
+  const uint32_t xmmupnu = (uint32_t)(s + dnmu + upnu) >> 1;                               // par
+  const uint32_t xmmumnu = (uint32_t)(s + dnmu + dnnu) >> 1;                               // par
+  const uint32_t xpmumnu = (uint32_t)(s + upmu + dnnu) >> 1;                               // par
+  m3<R> C;
+  {
+    const m3<R> P1 = prod_nn<LF, R>(lead<LF, R>(f, mu, par, i), f.template load<R>(nu, opp, xpmu));
+    const m3<R> P2 = prod_nn<LF, R>(lead<LF, R>(f, nu, par, i), f.template load<R>(mu, opp, xpnu));
+    C = mul_na(P1, P2);
+  }
+  {
+    const m3<R> S = prod_nn<LF, R>(lead<LF, R>(f, nu, opp, xmmu), f.template load<R>(mu, par, xmmupnu));
+    const m3<R> T = prod_na<LF, R>(lead<LF, R>(f, nu, par, i), S);
+    acc_nn(C, T, f.template load<R>(mu, opp, xmmu));
+  }
+  {
+    const m3<R> S1 = prod_nn<LF, R>(lead<LF, R>(f, nu, par, xmmumnu), f.template load<R>(mu, opp, xmmu));
+    const m3<R> S2 = prod_nn<LF, R>(lead<LF, R>(f, mu, par, xmmumnu), f.template load<R>(nu, opp, xmnu));
+    acc_an(C, S1, S2);
+  }
+  {
+    // rows 0 and 1 of S suffice for T = S U_mu(x)^dag
+    m3<R> S;
+    if constexpr (LF::NREAL == 12)
+      S = mul_nn_rows01(f.template load_rows01<R>(mu, opp, xmnu), f.template load<R>(nu, par, xpmumnu));
+    else
+      S = mul_nn(f.template load<R>(mu, opp, xmnu), f.template load<R>(nu, par, xpmumnu));
+    const m3<R> T = prod_na<LF, R>(S, f.template load<R>(mu, par, i));
+    acc_an(C, f.template load<R>(nu, opp, xmnu), T);
+  }
+  *out = ah_from_clover(C);
 }
 
 // Per-site unscaled clover sums: q_site = tr F01 F23 - tr F02 F13 + tr F03 F12 and
 // e_site = sum_{mu<nu} |F_mu nu|^2 (the 1/(4 pi^2) and 1/2 are applied to the totals).
 template <typename F, typename R>
 __device__ __forceinline__ void site_qe(const Geom& g, const F& f, const Coord& x, int par, uint32_t i, R* q, R* e) {
-  ah9<R> a, b;
-  clover_plane<F, R, 0, 1>(g, f, x, par, i, &a);
-  clover_plane<F, R, 2, 3>(g, f, x, par, i, &b);
-  R qs = re_tr_ah(a, b), es = sqnorm_ah(a) + sqnorm_ah(b);
-  clover_plane<F, R, 0, 2>(g, f, x, par, i, &a);
-  clover_plane<F, R, 1, 3>(g, f, x, par, i, &b);
-  qs -= re_tr_ah(a, b);
-  es += sqnorm_ah(a) + sqnorm_ah(b);
-  clover_plane<F, R, 0, 3>(g, f, x, par, i, &a);
-  clover_plane<F, R, 1, 2>(g, f, x, par, i, &b);
-  qs += re_tr_ah(a, b);
-  es += sqnorm_ah(a) + sqnorm_ah(b);
+  const NbOff o = nb_offsets(g, x);
+  R qs = 0, es = 0;
+#pragma unroll 1
+  for (int p = 0; p < 3; ++p) {
+    // pairs (01, 23), (02, 13), (03, 12) with signs +, -, +
+    const int nu1 = p + 1;
+    const int mu2 = (p == 0) ? 2 : 1;
+    const int nu2 = (p == 2) ? 2 : 3;
+    ah9<R> a, b;
+    clover_plane_rt<F, R>(f, x.s, o, 0, nu1, par, i, &a);
+    clover_plane_rt<F, R>(f, x.s, o, mu2, nu2, par, i, &b);
+    const R t = re_tr_ah(a, b);
+    qs += (p == 1) ? -t : t;
+    es += sqnorm_ah(a) + sqnorm_ah(b);
+  }
   *q += qs;
   *e += es;
 }

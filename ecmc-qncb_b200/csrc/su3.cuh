@@ -7,10 +7,6 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#ifndef QCB_PACKED_FP32
-#define QCB_PACKED_FP32 0
-#endif
-
 namespace qcb {
 
 template <typename R>
@@ -73,36 +69,6 @@ __device__ __forceinline__ cx<R> cfma_cc(cx<R> a, cx<R> b, cx<R> acc) {
   acc.im = fma(-a.im, b.re, acc.im);
   return acc;
 }
-
-#if QCB_PACKED_FP32
-// FP32 complex multiply-adds as two packed FP32 FMAs (__ffma2_rn, sm_100): lane 0 carries the
-// real part, lane 1 the imaginary part.  Each lane performs the same two fused operations in
-// the same order as the scalar forms above, so the results are bit-identical to them.
-template <>
-__device__ __forceinline__ cx<float> cfma(cx<float> a, cx<float> b, cx<float> acc) {
-  float2 r = __ffma2_rn(make_float2(a.re, a.re), make_float2(b.re, b.im), make_float2(acc.re, acc.im));
-  r = __ffma2_rn(make_float2(-a.im, a.im), make_float2(b.im, b.re), r);
-  return mk(r.x, r.y);
-}
-template <>
-__device__ __forceinline__ cx<float> cfma_cn(cx<float> a, cx<float> b, cx<float> acc) {
-  float2 r = __ffma2_rn(make_float2(a.re, a.re), make_float2(b.re, b.im), make_float2(acc.re, acc.im));
-  r = __ffma2_rn(make_float2(a.im, -a.im), make_float2(b.im, b.re), r);
-  return mk(r.x, r.y);
-}
-template <>
-__device__ __forceinline__ cx<float> cfma_nc(cx<float> a, cx<float> b, cx<float> acc) {
-  float2 r = __ffma2_rn(make_float2(a.re, -a.re), make_float2(b.re, b.im), make_float2(acc.re, acc.im));
-  r = __ffma2_rn(make_float2(a.im, a.im), make_float2(b.im, b.re), r);
-  return mk(r.x, r.y);
-}
-template <>
-__device__ __forceinline__ cx<float> cfma_cc(cx<float> a, cx<float> b, cx<float> acc) {
-  float2 r = __ffma2_rn(make_float2(a.re, -a.re), make_float2(b.re, b.im), make_float2(acc.re, acc.im));
-  r = __ffma2_rn(make_float2(-a.im, -a.im), make_float2(b.im, b.re), r);
-  return mk(r.x, r.y);
-}
-#endif
 
 template <typename R>
 struct m3 {
@@ -431,7 +397,28 @@ __device__ __forceinline__ m3<R> exp_su3(const alg8<R>& x) {
     q1i = n1i;
   }
   m3<R> X = alg_to_m3(x);
-  m3<R> X2 = mul_nn(X, X);
+  // X^2 is Hermitian (X^dag = -X); its entries in closed form from the 8 reals
+  // (d2 = -d0 - d1; a = X01, b = X02, c = X12):
+  //   (X^2)_kk = -(d_k^2 + sum of |off-diagonal|^2 in row k),
+  //   (X^2)_01 = -i d2 a - b c*, (X^2)_02 = -i d1 b + a c, (X^2)_12 = -i d0 c - a* b.
+  m3<R> X2;
+  {
+    const R D0 = x.a[0], D1 = x.a[1], D2 = -(x.a[0] + x.a[1]);
+    const R Ar = x.a[2], Ai = x.a[3], Br = x.a[4], Bi = x.a[5], Cr = x.a[6], Ci = x.a[7];
+    const R na = Ar * Ar + Ai * Ai, nb = Br * Br + Bi * Bi, nc = Cr * Cr + Ci * Ci;
+    X2.e[0][0] = mk<R>(-(D0 * D0 + na + nb), R(0));
+    X2.e[1][1] = mk<R>(-(D1 * D1 + na + nc), R(0));
+    X2.e[2][2] = mk<R>(-(D2 * D2 + nb + nc), R(0));
+    const cx<R> s01 = mk<R>(D2 * Ai - (Br * Cr + Bi * Ci), -D2 * Ar - (Bi * Cr - Br * Ci));
+    const cx<R> s02 = mk<R>(D1 * Bi + Ar * Cr - Ai * Ci, -D1 * Br + Ar * Ci + Ai * Cr);
+    const cx<R> s12 = mk<R>(D0 * Ci - (Ar * Br + Ai * Bi), -D0 * Cr - (Ar * Bi - Ai * Br));
+    X2.e[0][1] = s01;
+    X2.e[0][2] = s02;
+    X2.e[1][2] = s12;
+    X2.e[1][0] = conj(s01);
+    X2.e[2][0] = conj(s02);
+    X2.e[2][1] = conj(s12);
+  }
   cx<R> q0 = mk<R>(R(q0r), R(q0i)), q1 = mk<R>(R(q1r), R(q1i)), q2 = mk<R>(R(q2r), R(q2i));
   m3<R> E;
 #pragma unroll
