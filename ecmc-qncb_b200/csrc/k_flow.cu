@@ -17,21 +17,28 @@
 namespace qcb {
 
 // Grid (2 * tiles, 4): blockIdx.y = mu, blockIdx.x = 2 * tile + parity.  Blocks are issued
-// x-fastest, so one direction runs at a time (one mu instantiation in the instruction
-// cache) and both parities of a tile run together.  Measured on 32^4 per RK3 step, against
-// a mu-major parity-major grid and against a run-time-mu kernel with all eight (mu, parity)
-// blocks of a tile adjacent: FP32-12 1.44 vs 1.49 vs 1.58 ms; FP64-18 3.09 vs 3.77 vs 3.18 ms.
+// x-fastest, so one direction runs at a time over the whole lattice (one mu instantiation in
+// the instruction cache) and both parities of a tile run together.  Measured per RK3 step on
+// 32^4 FP32-12: 1.37 ms; a run-time-mu kernel with the eight (mu, parity) blocks of a tile
+// adjacent: 1.58 ms; chunks of 256 / 512 / 1024 tiles with the four directions of a chunk in
+// turn (to reuse the chunk's links from L2): 1.48 / 1.71 / 1.54 ms, because the direction
+// changes every one or two waves of blocks and the four instantiations then compete for the
+// instruction cache.  The flow is bound by instruction issue, not by DRAM.
+#ifndef QCB_FLOW_MINB32
+#define QCB_FLOW_MINB32 1
+#endif
 template <typename S, int NR, int STAGE>
-__global__ void __launch_bounds__(128) k_flow_stage(Geom g, Links<S, NR> src, Links<S, NR> dst, AlgField<S> acc,
+__global__ void __launch_bounds__(128, sizeof(S) == 4 ? QCB_FLOW_MINB32 : 1) k_flow_stage(Geom g, Links<S, NR> src, Links<S, NR> dst, AlgField<S> acc,
                                                     S eps) {
+  const int mu = blockIdx.y;
   const uint32_t i = (blockIdx.x >> 1) * blockDim.x + threadIdx.x;
   const int par = blockIdx.x & 1;
   if (i >= g.Vh) return;
-  switch (blockIdx.y) {
-    case 0: flow_link<Links<S, NR>, AlgField<S>, S, STAGE, 0>(g, src, dst, acc, eps, par, i); break;
-    case 1: flow_link<Links<S, NR>, AlgField<S>, S, STAGE, 1>(g, src, dst, acc, eps, par, i); break;
-    case 2: flow_link<Links<S, NR>, AlgField<S>, S, STAGE, 2>(g, src, dst, acc, eps, par, i); break;
-    default: flow_link<Links<S, NR>, AlgField<S>, S, STAGE, 3>(g, src, dst, acc, eps, par, i); break;
+  switch (mu) {
+    case 0: flow_link<Links<S, NR>, AlgField<S>, S, 0>(g, src, dst, acc, eps, STAGE, par, i); break;
+    case 1: flow_link<Links<S, NR>, AlgField<S>, S, 1>(g, src, dst, acc, eps, STAGE, par, i); break;
+    case 2: flow_link<Links<S, NR>, AlgField<S>, S, 2>(g, src, dst, acc, eps, STAGE, par, i); break;
+    default: flow_link<Links<S, NR>, AlgField<S>, S, 3>(g, src, dst, acc, eps, STAGE, par, i); break;
   }
 }
 

@@ -20,9 +20,12 @@ namespace qcb {
 
 // Blocks of 128 threads.  Resident blocks per SM (the register bound): FP32 5 (96
 // registers, measured 2.6% faster than 4 on 32^4), FP64 4 (a tighter bound spills).
+#ifndef QCB_HB_MINB32
+#define QCB_HB_MINB32 5
+#endif
 template <typename S>
 struct HbMinBlocks {
-  static constexpr int value = sizeof(S) == 4 ? 5 : 4;
+  static constexpr int value = sizeof(S) == 4 ? QCB_HB_MINB32 : 4;
 };
 
 // Frozen links of the reference's block decomposition (src/geometry/GeometryCB.cpp:33-56)

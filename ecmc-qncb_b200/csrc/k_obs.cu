@@ -93,8 +93,10 @@ __global__ void __launch_bounds__(RED_THREADS, RedMinBlocks<S>::value) k_plaquet
   double acc = 0.0;
   const uint64_t n = (uint64_t)g.V;
   for (uint64_t t = (uint64_t)blockIdx.x * RED_THREADS + threadIdx.x; t < n; t += (uint64_t)gridDim.x * RED_THREADS) {
-    const int par = (t >= g.Vh) ? 1 : 0;
-    const uint32_t i = (uint32_t)(t - (par ? g.Vh : 0));
+    // both parities of a checkerboard index together: a site's neighbours (opposite
+    // parity) are then read close in time, from L2
+    const int par = (int)(t & 1);
+    const uint32_t i = (uint32_t)(t >> 1);
     const Coord x = cb_coord(g, par, i);
     acc += (double)site_plaquette<Links<S, NR>, S>(g, f, x, par, i);
   }
@@ -143,8 +145,10 @@ __global__ void __launch_bounds__(RED_THREADS, RedMinBlocks<S>::value) k_clover_
   double accq = 0.0, acce = 0.0;
   const uint64_t n = (uint64_t)g.V;
   for (uint64_t t = (uint64_t)blockIdx.x * RED_THREADS + threadIdx.x; t < n; t += (uint64_t)gridDim.x * RED_THREADS) {
-    const int par = (t >= g.Vh) ? 1 : 0;
-    const uint32_t i = (uint32_t)(t - (par ? g.Vh : 0));
+    // both parities of a checkerboard index together: a site's neighbours (opposite
+    // parity) are then read close in time, from L2
+    const int par = (int)(t & 1);
+    const uint32_t i = (uint32_t)(t >> 1);
     const Coord x = cb_coord(g, par, i);
     R q = 0, e = 0;
     site_qe<Links<S, NR>, R>(g, f, x, par, i, &q, &e);
