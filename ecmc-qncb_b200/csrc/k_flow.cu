@@ -24,8 +24,10 @@ namespace qcb {
 // turn (to reuse the chunk's links from L2): 1.48 / 1.71 / 1.54 ms, because the direction
 // changes every one or two waves of blocks and the four instantiations then compete for the
 // instruction cache.  The flow is bound by instruction issue, not by DRAM.
+// Resident blocks per SM in FP32 (the register bound): 5 (96 registers) measured 1.36 ms
+// per RK3 step on 32^4 FP32-12 against 1.74 ms with the compiler's own choice.
 #ifndef QCB_FLOW_MINB32
-#define QCB_FLOW_MINB32 1
+#define QCB_FLOW_MINB32 5
 #endif
 template <typename S, int NR, int STAGE>
 __global__ void __launch_bounds__(128, sizeof(S) == 4 ? QCB_FLOW_MINB32 : 1) k_flow_stage(Geom g, Links<S, NR> src, Links<S, NR> dst, AlgField<S> acc,
