@@ -26,8 +26,12 @@ LIB = PKG / "lib" / "libqcb.so"
 DRIVER = PKG / "bin" / "gauge_hb_ncb"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# -prec-div=false / -prec-sqrt=false: FP32 division and square root by the hardware
+# approximations (a few ulp) instead of the IEEE-rounded sequences; FP64 is unaffected.  The
+# FP32 heatbath pass is 5% faster with them (the KP draw's divisions and roots); the FP32 flow
+# results are unchanged.
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
-              "--expt-relaxed-constexpr", "-I", str(INCLUDE)] + ARCH
+              "--expt-relaxed-constexpr", "-prec-div=false", "-prec-sqrt=false", "-I", str(INCLUDE)] + ARCH
 DRIVER_SOURCES = {"gauge_hb_ncb.cpp"}
 
 
