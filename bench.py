@@ -297,6 +297,11 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         result["serving"] = serving_section(ctx)
         result["latency"] = {"p50_s": result["serving"]["p50_s"], "p99_s": result["serving"]["p99_s"],
                              "workload": "serving stream (config 4)"}
+        # The 20 req/s stream offers about three times the work the GPU completes per second,
+        # so its latency is set by the queue.  The same job mix at 80% of the measured job
+        # throughput shows the latency of a server that keeps up.
+        rate = 0.8 * result["serving"]["throughput_jobs_per_s"]
+        result["serving_80pct_load"] = serving_section(ctx, n_requests=40, rate=rate)
     return result
 
 
@@ -565,13 +570,14 @@ def _ref_worker(args):
 
 
 def cpu_baseline(sweeps: int = 1, rk3: int = 1, block: int = 16):
-    """Reference algorithm on the host cores: one process per core (the reference runs
-    one MPI rank per core), each on a 16^4 block of the 32^4 lattice."""
+    """Reference algorithm on the host cores: one process per hardware thread (the reference
+    runs one MPI rank per core), each on a 16^4 block as in the reference's 2^4-rank
+    decomposition of 32^4; the rates are summed over the processes."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
 
     oracle.build()
-    cores = min(16, os.cpu_count() or 1)
+    cores = min(64, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1))
     with mp.get_context("spawn").Pool(cores) as pool:
         t = time.perf_counter()
         res = pool.map(_ref_worker, [(block, sweeps, rk3, 100 + r) for r in range(cores)])

@@ -185,6 +185,44 @@ def test_heatbath_fp32_tracks_fp64(ctx, prec, nr):
     assert abs(qcb.observables.mean_plaquette_global(f) - orc.plaquette(ref, dims)) < 1e-3
 
 
+def test_heatbath_fp64_12_matches_oracle(ctx):
+    """12-real FP64 storage: rows 0 and 1 stored, row 2 rebuilt, links re-orthonormalised in
+    FP64 after each update; the chain stays on the oracle's to 1e-10."""
+    dims = (4, 4, 6, 4)
+    u = orc.hot_philox(dims, 33)
+    f = lattice(ctx, u, dims, "fp64", 12)
+    qcb._lib.check(qcb._lib.lib().qcb_heatbath(f.h, 5.9, 2, 1, 4242, 0))
+    ref, fails = orc.heatbath_cb(u, dims, 5.9, 2, 1, 4242, 0)
+    assert fails == 0
+    assert np.abs(f.get_links() - ref).max() < 1e-10
+
+
+def test_flow_fp64_12_matches_oracle(ctx):
+    dims = (4, 4, 4, 6)
+    u = heated(dims, 24)
+    f = lattice(ctx, u, dims, "fp64", 12)
+    qcb._lib.check(qcb._lib.lib().qcb_flow_steps(f.h, 0.02, 3))
+    assert np.abs(f.get_links() - orc.flow_steps(u, dims, 0.02, 3)).max() < 1e-12
+
+
+def test_fp32_flow_links_stay_unitary(ctx):
+    """FP32 links are re-orthonormalised in FP64 once per RK3 step, so 60 steps leave them
+    unitary to FP32 rounding."""
+    dims = (6, 6, 6, 6)
+    base = qcb.GaugeField(ctx, dims)
+    base.hot_start(5)
+    qcb._lib.check(qcb._lib.lib().qcb_heatbath(base.h, 6.0, 5, 1, 5, 0))
+    for nr in (12, 18):
+        f = qcb.GaugeField(ctx, dims, "fp32", nr)
+        f.copy_from(base)
+        qcb._lib.check(qcb._lib.lib().qcb_flow_steps(f.h, 0.02, 60))
+        m = f.get_links().reshape(-1, 3, 3)
+        dev = np.abs(m @ np.conj(np.transpose(m, (0, 2, 1))) - np.eye(3)).max()
+        assert dev < 2e-6, (nr, dev)
+        assert np.abs(np.linalg.det(m) - 1).max() < 2e-6
+        f.close()
+
+
 def test_kp_cap_reports_error(ctx):
     # beta -> 0 makes alpha tiny, so KP acceptance (~2 alpha) is far below 1/4096
     f = qcb.GaugeField(ctx, (4, 4, 4, 4))
@@ -254,6 +292,8 @@ def test_precision_fp32_flow_vs_fp64(ctx):
     r32 = qcb.observables.topo_charge_flowed(f32, gf, 6, 10).reshape(-1, 3)
     assert np.abs(r64[:, 1] - r32[:, 1]).max() < 1e-4
     assert np.abs(r64[:, 2] - r32[:, 2]).max() < 1e-4 * r64[:, 2].max()
+    # with the per-step FP64 re-orthonormalisation E tracks FP64 to about 1e-7 relative
+    assert (np.abs(r64[:, 2] - r32[:, 2]) / r64[:, 2]).max() < 1e-6
 
 
 def test_context_destroyed_before_its_lattices():
