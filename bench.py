@@ -395,7 +395,7 @@ def batch_section(ctx, lib, stream):
             "mean_plaquette": float(np.mean(plaq)), "mean_E_t2": float(np.mean(rec[:, -1, 2]))}
 
 
-def serving_section(ctx, n_requests=100, rate=20.0):
+def serving_section(ctx, n_requests=100, rate=20.0, quantum_sweeps=2, quantum_steps=4):
     """Serving workload: a Poisson stream (mean `rate` req/s, stream seed 77) of 70% Wilson-flow
     measurements to t ~ U[1, 6] and 30% generate-N-sweeps jobs with N ~ U[10, 200]; sizes
     16^4 (0.4), 24^4 (0.3), 32^4 (0.2), 48^4 (0.1); beta ~ U[5.8, 6.3]; FP32 12-real.  The
@@ -423,7 +423,7 @@ def serving_section(ctx, n_requests=100, rate=20.0):
         qcb._lib.check(lib.qcb_heatbath(f.h, float(betas[k]), 20, 1, 7000 + k, 0))
         fields.append(f)
     ctx.sync()
-    srv = qcb.Server(ctx, "fp32", 12, hbm_budget=48 << 30, quantum_sweeps=2, quantum_steps=4)
+    srv = qcb.Server(ctx, "fp32", 12, hbm_budget=48 << 30, quantum_sweeps=quantum_sweeps, quantum_steps=quantum_steps)
     submit_t = {}
 
     def feeder():
@@ -453,6 +453,7 @@ def serving_section(ctx, n_requests=100, rate=20.0):
     work_upd = sum((0 if kinds[k] else int(nsw[k])) * 4 * int(sizes[k]) ** 4 for k in range(n_requests))
     return {"workload": f"Poisson {rate} req/s, {n_requests} requests, 70% flow t~U[1,6], 30% N~U[10,200] sweeps, "
                         "sizes 16/24/32/48^4 (0.4/0.3/0.2/0.1), beta~U[5.8,6.3], fp32-12",
+            "quantum": {"sweeps": quantum_sweeps, "rk3_steps": quantum_steps},
             "all_ok": ok, "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()), "admission_wait_p99_s": float(np.percentile(wait, 99)),
             "throughput_jobs_per_s": len(res) / span, "span_s": span,

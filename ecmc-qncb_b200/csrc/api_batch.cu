@@ -497,6 +497,27 @@ int qcb_batch_run(qcb_batch* b, const qcb_batch_plan* plan, const double* betas,
   return QCB_OK;
 }
 
+int qcb_wait_selftest(qcb_ctx* ctx, double limit_s, uint32_t* timeouts, uint32_t* aborted) {
+  if (!ctx || !timeouts || !aborted) return bfail(QCB_ERR_INVALID, "null argument");
+  if (!(limit_s > 0.0 && limit_s <= 5.0)) return bfail(QCB_ERR_INVALID, "limit_s must be in (0, 5]");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  BCU(cudaSetDevice(ctx->device), "cudaSetDevice");
+  uint32_t* d = nullptr;  // [0] the flag nothing sets, [1..4] status words
+  BCU(cudaMalloc(&d, 8 * sizeof(uint32_t)), "self-test buffer");
+  uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  cudaError_t e = cudaMemsetAsync(d, 0, 8 * sizeof(uint32_t), ctx->stream);
+  if (e == cudaSuccess) e = launch_wait_probe(d, d + 1, (uint64_t)(limit_s * 1e9), 4, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return bcuda(e, "wait self-test");
+  ctx->launches++;
+  *timeouts = h[2];
+  *aborted = h[3];
+  if (h[4] != 0) return bfail(QCB_ERR_STATE, "a wait on a flag that nothing sets succeeded");
+  return QCB_OK;
+}
+
 }  // extern "C"
 
 // ---- autotuner --------------------------------------------------------------------------

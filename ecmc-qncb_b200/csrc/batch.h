@@ -44,6 +44,12 @@ enum : int { BATCH_NONE = -1, BATCH_HB = 0, BATCH_FLOW = 1, BATCH_MIXED = 2 };
 cudaError_t launch_batch(int kind, const BatchRun& run, int prec, int nr, int block, int max_blocks,
                          cudaStream_t s);
 
+// Bounded-wait self-test: `blocks` co-resident blocks wait on flag[0] (never set); block 0
+// gives up after limit_ns.  status[1] = timeouts, status[2] = abort flag, status[3] = waits
+// that succeeded.
+cudaError_t launch_wait_probe(const uint32_t* flag, uint32_t* status, uint64_t limit_ns, int blocks,
+                              cudaStream_t s);
+
 // Batched reductions: one item per (lattice, tile of RED sites), item r of lattice l in
 // [rprefix[l], rprefix[l+1]).  out[l] = mean plaquette; out2[2l], out2[2l+1] = (Q, E).
 // scratch holds 2 * rprefix[nlat] doubles.

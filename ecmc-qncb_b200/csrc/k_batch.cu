@@ -32,6 +32,9 @@
 namespace qcb {
 
 constexpr uint64_t WAIT_NS = 2000000000ull;  // 2 s per wait
+// Iteration bound of one wait, besides its time bound (a wait whose clock reads stall still
+// ends): far above the iterations of a 2 s wait of L2 round trips.
+constexpr uint64_t WAIT_MAX_ITERS = 1ull << 28;
 
 __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
   uint32_t v;
@@ -58,20 +61,22 @@ __device__ __forceinline__ int find_lattice(const uint32_t* __restrict__ prefix,
 }
 
 // Thread 0 waits until done[l] >= target; returns false (for the whole block) on abort
-// or timeout.  status[1] counts timeouts, status[2] is the abort flag.
-__device__ __forceinline__ bool block_wait(const uint32_t* done, uint32_t target, uint32_t* status) {
+// or timeout (limit_ns of wall-clock time or WAIT_MAX_ITERS polls).  status[1] counts
+// timeouts, status[2] is the abort flag.
+__device__ __forceinline__ bool block_wait(const uint32_t* done, uint32_t target, uint32_t* status,
+                                           uint64_t limit_ns = WAIT_NS) {
   __shared__ int ok;
   if (threadIdx.x == 0) {
     int res = 1;
     if (ld_acquire_u32(done) < target) {
       const uint64_t t0 = global_ns();
-      for (;;) {
+      for (uint64_t it = 0;; ++it) {
         if (ld_acquire_u32(done) >= target) break;
         if (ld_acquire_u32(&status[2])) {
           res = 0;
           break;
         }
-        if (global_ns() - t0 > WAIT_NS) {
+        if (global_ns() - t0 > limit_ns || it > WAIT_MAX_ITERS) {
           atomicAdd(&status[1], 1u);
           atomicExch(&status[2], 1u);
           res = 0;
@@ -207,6 +212,23 @@ cudaError_t launch_batch(int kind, const BatchRun& run, int prec, int nr, int bl
   if (block <= 0) block = 128;
   if (block > 128 || (block & 31)) return cudaErrorInvalidValue;
   QCB_DISPATCH_STORE(probe, batch_launch_impl, kind, run, block, max_blocks, s);
+}
+
+// ---- wait self-test -------------------------------------------------------------------------
+// Block 0 waits for flag[0] >= 1, which nothing sets, until its limit; it then counts a
+// timeout and raises the abort flag.  The other blocks wait for the same flag with a longer
+// limit and return when they see the abort flag.  Exercises the bounded wait and abort path
+// of the persistent kernels without a fault.
+__global__ void k_wait_probe(const uint32_t* flag, uint32_t* status, uint64_t limit_ns) {
+  const uint64_t lim = blockIdx.x == 0 ? limit_ns : 4 * limit_ns;
+  if (!block_wait(flag, 1u, status, lim)) return;
+  if (threadIdx.x == 0) atomicAdd(&status[3], 1u);  // a wait that succeeded (not expected)
+}
+
+cudaError_t launch_wait_probe(const uint32_t* flag, uint32_t* status, uint64_t limit_ns, int blocks,
+                              cudaStream_t s) {
+  void* args[] = {(void*)&flag, (void*)&status, (void*)&limit_ns};
+  return cudaLaunchCooperativeKernel((void*)k_wait_probe, dim3(blocks), dim3(32), args, 0, s);
 }
 
 // ---- batched observables --------------------------------------------------------------------

@@ -11,6 +11,24 @@
 
 namespace qcb {
 
+// Neighbour offsets of site x in every direction: up[d] = full-index step to x + d,
+// dn[d] = step to x - d (periodic).
+struct NbOff {
+  int32_t up[4], dn[4];
+};
+__device__ __forceinline__ NbOff nb_offsets(const Geom& g, const Coord& x) {
+  NbOff o;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    o.up[d] = (x.c[d] + 1 == g.L[d]) ? (1 - g.L[d]) * g.str[d] : g.str[d];
+    o.dn[d] = (x.c[d] == 0) ? (g.L[d] - 1) * g.str[d] : -g.str[d];
+  }
+  return o;
+}
+__device__ __forceinline__ int32_t sel4(const int32_t* v, int k) {
+  return k == 0 ? v[0] : (k == 1 ? v[1] : (k == 2 ? v[2] : v[3]));
+}
+
 // The two staple terms of one plane (mu, nu), added to A.  Site indices: i = x (parity
 // par); ixmu = x+mu, ixnu = x+nu, ixmnu = x-nu (parity opp); ixmunu = x+mu-nu (parity par).
 // With 12-real storage each three-link product is an SU(3) matrix whose third row follows
@@ -73,24 +91,6 @@ __device__ __forceinline__ m3<R> staple_sum(const Geom& g, const F& f, const Coo
     staple_terms<F, R>(A, f, nu, MU, par, opp, i, cb_index(xmu), cb_index(xnu), cb_index(xmunu), cb_index(xmnu));
   }
   return A;
-}
-
-// Neighbour offsets of site x in every direction: up[d] = full-index step to x + d,
-// dn[d] = step to x - d (periodic).
-struct NbOff {
-  int32_t up[4], dn[4];
-};
-__device__ __forceinline__ NbOff nb_offsets(const Geom& g, const Coord& x) {
-  NbOff o;
-#pragma unroll
-  for (int d = 0; d < 4; ++d) {
-    o.up[d] = (x.c[d] + 1 == g.L[d]) ? (1 - g.L[d]) * g.str[d] : g.str[d];
-    o.dn[d] = (x.c[d] == 0) ? (g.L[d] - 1) * g.str[d] : -g.str[d];
-  }
-  return o;
-}
-__device__ __forceinline__ int32_t sel4(const int32_t* v, int k) {
-  return k == 0 ? v[0] : (k == 1 ? v[1] : (k == 2 ? v[2] : v[3]));
 }
 
 // Same staple sum with the direction mu known only at run time: one code path for all

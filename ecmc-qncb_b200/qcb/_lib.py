@@ -131,6 +131,7 @@ SIGNATURES = {
     "qcb_server_stats_get": (C.c_int, [_vp, C.POINTER(ServerStats)]),
     "qcb_server_clock": (C.c_double, [_vp]),
     "qcb_server_destroy": (C.c_int, [_vp]),
+    "qcb_wait_selftest": (C.c_int, [_vp, C.c_double, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "qcb_params_default": (C.c_int, [C.POINTER(HbParams)]),
     "qcb_params_load": (C.c_int, [C.c_char_p, C.POINTER(HbParams)]),
 }

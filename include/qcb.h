@@ -216,6 +216,16 @@ int qcb_batch_run(qcb_batch* b, const qcb_batch_plan* plan, const double* betas,
  * NULL = no cache) under keys "<device name>|<precision>-<storage>|<hb|flow>|LxLyLzLt". */
 int qcb_batch_autotune(qcb_batch* b, const char* cache_path);
 
+/* ---- failure detection --------------------------------------------------------------
+ * The persistent batch and server kernels wait on per-lattice counters that other blocks
+ * advance; every wait is bounded (2 s of wall-clock time or 2^28 polls), after which the
+ * block counts a timeout, raises an abort flag that makes every block return, and the host
+ * reports QCB_ERR_CUDA with the count.  qcb_wait_selftest runs that path on purpose: four
+ * co-resident blocks wait on a device flag that nothing sets; the first gives up after
+ * limit_s (at most 5 s) and aborts the others.  On return *timeouts = 1 and *aborted = 1 and
+ * the context stays usable.  No GPU fault is involved. */
+int qcb_wait_selftest(qcb_ctx* ctx, double limit_s, uint32_t* timeouts, uint32_t* aborted);
+
 /* ---- serving ---------------------------------------------------------------------------
  * No counterpart in the reference.  A request server with continuous batching: jobs
  * (Wilson-flow measurements and generate-N-sweeps runs on resident lattices of any sizes)
