@@ -53,6 +53,13 @@ int qcb::check_status(qcb_ctx* c) {
      "status copy");
   CU(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
   uint32_t kp = c->h_status[0];
+  const uint32_t timeouts = c->h_status[1], aborted = c->h_status[2];
+  if (timeouts || aborted) {
+    CU(cudaMemsetAsync(c->d_status, 0, 4 * sizeof(uint32_t), c->stream), "status reset");
+    CU(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    return fail(QCB_ERR_CUDA, "a persistent kernel gave up waiting (" + std::to_string(timeouts) +
+                                  " wait timeout(s)); the launch was abandoned");
+  }
   if (kp) {
     CU(cudaMemsetAsync(c->d_status, 0, 4 * sizeof(uint32_t), c->stream), "status reset");
     CU(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");

@@ -22,6 +22,7 @@
 #include "flow_link.cuh"
 #include "hb_link.cuh"
 #include "obs_site.cuh"
+#include "sync.cuh"
 
 // Resident blocks of 128 threads per SM in FP32 (the register bound): 5 measured 10% (heatbath)
 // and 19% (flow) faster than 4 on the 64-lattice batch, 3 slower.
@@ -30,22 +31,6 @@
 #endif
 
 namespace qcb {
-
-constexpr uint64_t WAIT_NS = 2000000000ull;  // 2 s per wait
-// Iteration bound of one wait, besides its time bound (a wait whose clock reads stall still
-// ends): far above the iterations of a 2 s wait of L2 round trips.
-constexpr uint64_t WAIT_MAX_ITERS = 1ull << 28;
-
-__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
-  uint32_t v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
 
 // Decode item r (within one level) into (lattice, tile) by binary search of prefix[].
 __device__ __forceinline__ int find_lattice(const uint32_t* __restrict__ prefix, int nlat, uint32_t r) {
@@ -66,27 +51,7 @@ __device__ __forceinline__ int find_lattice(const uint32_t* __restrict__ prefix,
 __device__ __forceinline__ bool block_wait(const uint32_t* done, uint32_t target, uint32_t* status,
                                            uint64_t limit_ns = WAIT_NS) {
   __shared__ int ok;
-  if (threadIdx.x == 0) {
-    int res = 1;
-    if (ld_acquire_u32(done) < target) {
-      const uint64_t t0 = global_ns();
-      for (uint64_t it = 0;; ++it) {
-        if (ld_acquire_u32(done) >= target) break;
-        if (ld_acquire_u32(&status[2])) {
-          res = 0;
-          break;
-        }
-        if (global_ns() - t0 > limit_ns || it > WAIT_MAX_ITERS) {
-          atomicAdd(&status[1], 1u);
-          atomicExch(&status[2], 1u);
-          res = 0;
-          break;
-        }
-        __nanosleep(100);
-      }
-    }
-    ok = res;
-  }
+  if (threadIdx.x == 0) ok = wait_geq(done, target, status, limit_ns) ? 1 : 0;
   __syncthreads();
   const bool r = ok != 0;
   __syncthreads();
