@@ -298,6 +298,41 @@ int qcb_lattice_create(qcb_ctx* c, const int dims[4], int precision, int storage
   return QCB_OK;
 }
 
+int qcb_lattice_create_slab(qcb_ctx* c, const int global_dims[4], int t0, int t_local, int precision, int storage,
+                            qcb_lattice** out) {
+  CHECK_CTX(c);
+  if (!out) return fail(QCB_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  if (!valid_dims(global_dims)) return fail(QCB_ERR_INVALID, "lattice extents must be even, >= 2, volume < 2^30");
+  if (t_local < 2 || (t_local & 1) || (t0 & 1) || t0 < 0 || t0 + t_local > global_dims[3])
+    return fail(QCB_ERR_INVALID, "slab times must be even, t_local >= 2, t0 >= 0 and t0 + t_local <= Lt");
+  if (precision != QCB_FP64 && precision != QCB_FP32) return fail(QCB_ERR_INVALID, "bad precision");
+  if (storage != QCB_R18 && storage != QCB_R12) return fail(QCB_ERR_INVALID, "bad storage");
+  LOCK(c);
+  TRY(set_device(c));
+  qcb_lattice* L = new (std::nothrow) qcb_lattice();
+  if (!L) return fail(QCB_ERR_NOMEM, "host allocation failed");
+  L->ctx = c;
+  L->dev.g = make_slab_geom(global_dims, t0, t_local);
+  L->dev.prec = precision;
+  L->dev.nr = storage;
+  for (int d = 0; d < 4; ++d) L->gdims[d] = global_dims[d];
+  L->slab_t0 = t0;
+  L->slab_tl = t_local;
+  L->bytes = link_bytes(L->dev.g, precision, storage);
+  if (cudaMalloc(&L->dev.links, L->bytes) != cudaSuccess) {
+    cudaGetLastError();
+    delete L;
+    return fail(QCB_ERR_NOMEM, "cannot allocate " + std::to_string(L->bytes) + " bytes of link storage");
+  }
+  CU(cudaMemsetAsync(L->dev.links, 0, L->bytes, c->stream), "memset");
+  CU(launch_cold(L->dev, c->stream, 0), "cold start");
+  c->launches++;
+  c->refs++;
+  *out = L;
+  return QCB_OK;
+}
+
 int qcb_lattice_destroy(qcb_lattice* L) {
   if (!L) return QCB_OK;
   qcb_ctx* c = L->ctx;
@@ -373,6 +408,7 @@ int qcb_reunitarize(qcb_lattice* L) {
 
 int qcb_gauge_transform(qcb_lattice* L, uint64_t seed) {
   CHECK_LAT(L);
+  if (L->slab_tl) return fail(QCB_ERR_STATE, "not available on a slab (needs halo exchanges between its passes)");
   qcb_ctx* c = L->ctx;
   LOCK(c);
   TRY(set_device(c));
@@ -500,6 +536,7 @@ int qcb_ildg_probe(const char* path, uint64_t* data_offset, uint64_t* data_bytes
 
 int qcb_save_ildg(qcb_lattice* L, const char* path) {
   CHECK_LAT(L);
+  if (L->slab_tl) return fail(QCB_ERR_STATE, "not available on a slab (needs halo exchanges between its passes)");
   if (!path) return fail(QCB_ERR_INVALID, "null path");
   qcb_ctx* c = L->ctx;
   LOCK(c);
@@ -544,6 +581,7 @@ int qcb_save_ildg(qcb_lattice* L, const char* path) {
 
 int qcb_load_ildg(qcb_lattice* L, const char* path) {
   CHECK_LAT(L);
+  if (L->slab_tl) return fail(QCB_ERR_STATE, "not available on a slab (needs halo exchanges between its passes)");
   if (!path) return fail(QCB_ERR_INVALID, "null path");
   qcb_ctx* c = L->ctx;
   LOCK(c);
@@ -598,6 +636,7 @@ int qcb_load_ildg(qcb_lattice* L, const char* path) {
 // ---- heatbath ---------------------------------------------------------------------------------
 int qcb_heatbath(qcb_lattice* L, double beta, int n_sweeps, int n_hits, uint64_t seed, uint64_t sweep_offset) {
   CHECK_LAT(L);
+  if (L->slab_tl) return fail(QCB_ERR_STATE, "not available on a slab (needs halo exchanges between its passes)");
   if (n_sweeps < 0 || n_hits < 0) return fail(QCB_ERR_INVALID, "negative sweep or hit count");
   if (!(beta > 0.0)) return fail(QCB_ERR_INVALID, "beta must be positive");
   if (n_hits > (1 << 20)) return fail(QCB_ERR_INVALID, "too many hits");
@@ -619,6 +658,7 @@ int qcb_heatbath(qcb_lattice* L, double beta, int n_sweeps, int n_hits, uint64_t
 int qcb_heatbath_frozen(qcb_lattice* L, double beta, int n_sweeps, int n_hits, uint64_t seed, uint64_t sweep_offset,
                         int l_core, const int shift[4]) {
   CHECK_LAT(L);
+  if (L->slab_tl) return fail(QCB_ERR_STATE, "not available on a slab (needs halo exchanges between its passes)");
   if (n_sweeps < 0 || n_hits < 0) return fail(QCB_ERR_INVALID, "negative sweep or hit count");
   if (!(beta > 0.0)) return fail(QCB_ERR_INVALID, "beta must be positive");
   if (n_hits > (1 << 20)) return fail(QCB_ERR_INVALID, "too many hits");
@@ -645,6 +685,7 @@ int qcb_heatbath_frozen(qcb_lattice* L, double beta, int n_sweeps, int n_hits, u
 
 int qcb_translate(qcb_lattice* L, const int shift[4]) {
   CHECK_LAT(L);
+  if (L->slab_tl) return fail(QCB_ERR_STATE, "not available on a slab (needs halo exchanges between its passes)");
   if (!shift) return fail(QCB_ERR_INVALID, "null shift");
   int sh[4];
   for (int d = 0; d < 4; ++d) sh[d] = ((shift[d] % L->dev.g.L[d]) + L->dev.g.L[d]) % L->dev.g.L[d];
@@ -670,7 +711,7 @@ int qcb_plaquette(qcb_lattice* L, double* out) {
   c->launches += 2;
   CU(cudaMemcpyAsync(c->h_out, c->d_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H");
   TRY(check_status(c));
-  *out = c->h_out[0] / (6.0 * (double)L->dev.g.V);
+  *out = c->h_out[0] / (6.0 * (double)L->dev.g.Vg);
   return QCB_OK;
 }
 
@@ -691,6 +732,7 @@ int qcb_topo_qe(qcb_lattice* L, double* q, double* e) {
 // ---- Wilson flow --------------------------------------------------------------------------
 int qcb_flow_measure(qcb_lattice* L, double eps, int n_steps_gf, int n_rk_steps, double* tQE) {
   CHECK_LAT(L);
+  if (L->slab_tl) return fail(QCB_ERR_STATE, "not available on a slab (needs halo exchanges between its passes)");
   if (n_steps_gf < 0 || n_rk_steps < 0) return fail(QCB_ERR_INVALID, "negative step count");
   if (n_steps_gf > 0 && !tQE) return fail(QCB_ERR_INVALID, "null output");
   qcb_ctx* c = L->ctx;
@@ -730,6 +772,7 @@ int qcb_flow_measure(qcb_lattice* L, double eps, int n_steps_gf, int n_rk_steps,
 
 int qcb_flow_steps(qcb_lattice* L, double eps, int n) {
   CHECK_LAT(L);
+  if (L->slab_tl) return fail(QCB_ERR_STATE, "not available on a slab (needs halo exchanges between its passes)");
   if (n < 0) return fail(QCB_ERR_INVALID, "negative step count");
   qcb_ctx* c = L->ctx;
   LOCK(c);
@@ -747,6 +790,164 @@ int qcb_flow_steps(qcb_lattice* L, double eps, int n) {
   }
   if (a.links != L->dev.links)
     CU(cudaMemcpyAsync(L->dev.links, a.links, L->bytes, cudaMemcpyDeviceToDevice, c->stream), "D2D copy");
+  return QCB_OK;
+}
+
+// ---- slabs: one pass / one stage at a time, halo exchange --------------------------------------
+int qcb_heatbath_pass(qcb_lattice* L, int mu, int parity, double beta, int n_hits, uint64_t seed, uint64_t sweep) {
+  CHECK_LAT(L);
+  if (mu < 0 || mu > 3 || (parity != 0 && parity != 1)) return fail(QCB_ERR_INVALID, "bad direction or parity");
+  if (n_hits < 0 || n_hits > (1 << 20)) return fail(QCB_ERR_INVALID, "bad hit count");
+  if (!(beta > 0.0)) return fail(QCB_ERR_INVALID, "beta must be positive");
+  qcb_ctx* c = L->ctx;
+  LOCK(c);
+  TRY(set_device(c));
+  // local time = global time - t0 + 1, so local parity = global parity + (1 - t0) (mod 2)
+  const int local_par = L->slab_tl ? (parity ^ ((L->slab_t0 + 1) & 1)) : parity;
+  CU(launch_hb_pass(L->dev, mu, local_par, beta, seed, (uint32_t)sweep, n_hits, c->d_status, c->stream, c->block),
+     "heatbath pass");
+  c->launches++;
+  return QCB_OK;
+}
+
+int qcb_flow_stage(qcb_lattice* L, int stage, double eps, int step) {
+  CHECK_LAT(L);
+  if (stage < 1 || stage > 3 || step < 0) return fail(QCB_ERR_INVALID, "bad stage or step");
+  qcb_ctx* c = L->ctx;
+  LOCK(c);
+  TRY(set_device(c));
+  TRY(ensure_flow_space(L));
+  // step s ping-pongs between the links (a) and the work buffer fw[0] (b) as qcb_flow_steps:
+  // stage 1 a -> b, stage 2 b -> a, stage 3 a -> b, with a and b swapped for odd s
+  const LatDev x = L->dev, y = with_links(L->dev, L->fw[0]);
+  const LatDev& a = (step & 1) ? y : x;
+  const LatDev& b = (step & 1) ? x : y;
+  AlgDev z;
+  z.p = L->fz;
+  const LatDev& src = (stage == 2) ? b : a;
+  const LatDev& dst = (stage == 2) ? a : b;
+  CU(launch_flow_stage(stage, src, dst, z, eps, c->stream, c->block), "flow stage");
+  c->launches++;
+  return QCB_OK;
+}
+
+int qcb_flow_finish(qcb_lattice* L, int n_steps) {
+  CHECK_LAT(L);
+  if (n_steps < 0) return fail(QCB_ERR_INVALID, "negative step count");
+  if (!(n_steps & 1)) return QCB_OK;  // the result is already in the links
+  qcb_ctx* c = L->ctx;
+  LOCK(c);
+  TRY(set_device(c));
+  if (!L->fw[0]) return fail(QCB_ERR_STATE, "no flow stage has run on this lattice");
+  CU(cudaMemcpyAsync(L->dev.links, L->fw[0], L->bytes, cudaMemcpyDeviceToDevice, c->stream), "D2D copy");
+  return QCB_OK;
+}
+
+namespace {
+// Device pointers of one face of a slab: the NC chunk segments of time slice `slice` for
+// links (mu, local parity par) of buffer `which` (0 links, 1 flow work buffer).
+int face_segments(qcb_lattice* L, int which, int slice, int mu, int par, char** seg, size_t* bytes, int* nseg) {
+  const Geom& g = L->dev.g;
+  const int prec_bytes = (L->dev.prec == QCB_FP64) ? 8 : 4;
+  const int nc = (L->dev.prec == QCB_FP32 && L->dev.nr == 12) ? 3 : (L->dev.nr == 12 ? 6 : 9);
+  const size_t vbytes = (size_t)prec_bytes * (size_t)L->dev.nr / (size_t)nc;  // bytes of one chunk element
+  char* base = (char*)(which == 0 ? L->dev.links : L->fw[0]);
+  if (!base) return fail(QCB_ERR_STATE, "the flow work buffer does not exist yet");
+  const size_t half = (size_t)g.str[3] / 2;  // checkerboard sites of one parity in one time slice
+  for (int c = 0; c < nc; ++c)
+    seg[c] = base + (((size_t)((mu * 2 + par) * nc + c)) * g.stride + (size_t)slice * half) * vbytes;
+  *bytes = half * vbytes;
+  *nseg = nc;
+  return QCB_OK;
+}
+}  // namespace
+
+int qcb_slab_info(const qcb_lattice* L, int global_dims[4], int* t0, int* t_local) {
+  CHECK_LAT(L);
+  if (global_dims)
+    for (int d = 0; d < 4; ++d) global_dims[d] = L->slab_tl ? L->gdims[d] : L->dev.g.L[d];
+  if (t0) *t0 = L->slab_t0;
+  if (t_local) *t_local = L->slab_tl;
+  return QCB_OK;
+}
+
+int qcb_slab_face(qcb_lattice* L, int which, int side, int mu, int parity, void** segments, size_t* bytes,
+                  int* n_segments) {
+  CHECK_LAT(L);
+  if (!L->slab_tl) return fail(QCB_ERR_STATE, "not a slab");
+  if (which < 0 || which > 1 || side < 0 || side > 3 || mu < 0 || mu > 3 || (parity != 0 && parity != 1) ||
+      !segments || !bytes || !n_segments)
+    return fail(QCB_ERR_INVALID, "bad face arguments");
+  const int slice = (side == 0) ? 0 : (side == 1) ? 1 : (side == 2) ? L->slab_tl : L->slab_tl + 1;
+  const int par = parity ^ ((L->slab_t0 + 1) & 1);
+  char* seg[9];
+  TRY(face_segments(L, which, slice, mu, par, seg, bytes, n_segments));
+  for (int c = 0; c < *n_segments; ++c) segments[c] = seg[c];
+  return QCB_OK;
+}
+
+int qcb_slab_face_copy(qcb_lattice* L, int which, int side, int mu, int parity, void* buf, int to_face) {
+  CHECK_LAT(L);
+  if (!buf) return fail(QCB_ERR_INVALID, "null buffer");
+  void* seg[9];
+  size_t nb = 0;
+  int ns = 0;
+  TRY(qcb_slab_face(L, which, side, mu, parity, seg, &nb, &ns));
+  qcb_ctx* c = L->ctx;
+  LOCK(c);
+  TRY(set_device(c));
+  char* b = (char*)buf;
+  for (int k = 0; k < ns; ++k) {
+    if (to_face)
+      CU(cudaMemcpyAsync(seg[k], b + (size_t)k * nb, nb, cudaMemcpyDefault, c->stream), "face copy");
+    else
+      CU(cudaMemcpyAsync(b + (size_t)k * nb, seg[k], nb, cudaMemcpyDefault, c->stream), "face copy");
+  }
+  CU(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  return QCB_OK;
+}
+
+int qcb_slab_exchange(qcb_lattice* lower, qcb_lattice* upper, int which, int mu, int parity) {
+  if (!lower || !upper) return fail(QCB_ERR_INVALID, "null lattice");
+  if (!lower->slab_tl || !upper->slab_tl) return fail(QCB_ERR_STATE, "not a slab");
+  for (int d = 0; d < 4; ++d)
+    if (lower->gdims[d] != upper->gdims[d]) return fail(QCB_ERR_INVALID, "slabs of different lattices");
+  if (lower->dev.prec != upper->dev.prec || lower->dev.nr != upper->dev.nr)
+    return fail(QCB_ERR_INVALID, "slabs of different storage");
+  if ((lower->slab_t0 + lower->slab_tl) % lower->gdims[3] != upper->slab_t0)
+    return fail(QCB_ERR_INVALID, "upper slab does not follow lower slab in time");
+  if (which < 0 || which > 1 || mu < -1 || mu > 3 || parity < -1 || parity > 1)
+    return fail(QCB_ERR_INVALID, "bad exchange arguments");
+  qcb_ctx* cl = lower->ctx;
+  qcb_ctx* cu = upper->ctx;
+  // both slabs' work must be done before their faces move; copies run on the lower stream
+  {
+    LOCK(cu);
+    CU(cudaSetDevice(cu->device), "cudaSetDevice");
+    CU(cudaStreamSynchronize(cu->stream), "cudaStreamSynchronize");
+  }
+  LOCK(cl);
+  TRY(set_device(cl));
+  CU(cudaStreamSynchronize(cl->stream), "cudaStreamSynchronize");
+  for (int m = 0; m < 4; ++m) {
+    if (mu >= 0 && m != mu) continue;
+    for (int p = 0; p < 2; ++p) {
+      if (parity >= 0 && p != parity) continue;
+      char *lo_last[9], *lo_halo[9], *up_first[9], *up_halo[9];
+      size_t nb = 0;
+      int ns = 0;
+      const int lp = p ^ ((lower->slab_t0 + 1) & 1), up = p ^ ((upper->slab_t0 + 1) & 1);
+      TRY(face_segments(lower, which, lower->slab_tl, m, lp, lo_last, &nb, &ns));
+      TRY(face_segments(lower, which, lower->slab_tl + 1, m, lp, lo_halo, &nb, &ns));
+      TRY(face_segments(upper, which, 1, m, up, up_first, &nb, &ns));
+      TRY(face_segments(upper, which, 0, m, up, up_halo, &nb, &ns));
+      for (int k = 0; k < ns; ++k) {
+        CU(cudaMemcpyPeerAsync(up_halo[k], cu->device, lo_last[k], cl->device, nb, cl->stream), "face copy");
+        CU(cudaMemcpyPeerAsync(lo_halo[k], cl->device, up_first[k], cu->device, nb, cl->stream), "face copy");
+      }
+    }
+  }
+  CU(cudaStreamSynchronize(cl->stream), "cudaStreamSynchronize");
   return QCB_OK;
 }
 

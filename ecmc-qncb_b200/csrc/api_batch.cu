@@ -288,6 +288,7 @@ int qcb_batch_create(qcb_ctx* ctx, int n, qcb_lattice* const* lats, qcb_batch** 
   *out = nullptr;
   for (int l = 0; l < n; ++l) {
     if (!lats[l]) return bfail(QCB_ERR_INVALID, "null lattice in batch");
+    if (lats[l]->slab_tl) return bfail(QCB_ERR_INVALID, "a slab cannot join a batch (it needs halo exchanges)");
     if (lats[l]->ctx != ctx) return bfail(QCB_ERR_INVALID, "batch lattices must share the context");
     if (lats[l]->dev.prec != lats[0]->dev.prec || lats[l]->dev.nr != lats[0]->dev.nr)
       return bfail(QCB_ERR_INVALID, "batch lattices must share precision and storage");

@@ -64,6 +64,7 @@ template <typename F, typename ACC, typename R, int MU>
 __device__ __forceinline__ void flow_link(const Geom& g, const F& src, const F& dst, const ACC& acc, R eps, int stage,
                                           int par, uint32_t i) {
   const Coord x = cb_coord(g, par, i);
+  if (!own_site(g, x.c[3])) return;  // halo slice of a slab
   const m3<R> A = staple_sum<F, R, MU>(g, src, x, par, i);
   const m3<R> U = src.template load<R>(MU, par, i);
   // Z = P_TA(-U A) = -P_TA(U A)
@@ -82,6 +83,7 @@ template <typename F, typename ACC, typename R>
 __device__ __forceinline__ void flow_link_rt(const Geom& g, const F& src, const F& dst, const ACC& acc, R eps, int stage,
                                              int mu, int par, uint32_t i) {
   const Coord x = cb_coord(g, par, i);
+  if (!own_site(g, x.c[3])) return;  // halo slice of a slab
   const m3<R> A = staple_sum_rt<F, R>(g, src, x, mu, par, i);
   const m3<R> U = src.template load<R>(mu, par, i);
   alg8<R> Z = proj_ta(mul_nn(U, A));

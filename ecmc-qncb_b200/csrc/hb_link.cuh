@@ -151,9 +151,10 @@ template <typename F, typename R, int NR, int MU>
 __device__ __forceinline__ uint32_t hb_update_link(const Geom& g, const F& f, int par, uint32_t i, R beta,
                                                    uint32_t k0, uint32_t k1, uint32_t sweep, int n_hits) {
   const Coord x = cb_coord(g, par, i);
+  if (!own_site(g, x.c[3])) return 0;  // halo slice of a slab
   const m3<R> A = staple_sum<F, R, MU>(g, f, x, par, i);
   m3<R> U = f.template load<R>(MU, par, i);
-  const uint32_t link = (uint32_t)MU * g.V + x.s;
+  const uint32_t link = (uint32_t)MU * g.Vg + (x.s + g.soff);
   uint32_t fails = 0;
   for (int h = 0; h < n_hits; ++h) {
     const uint32_t hb = RNG_DOMAIN_HB | ((uint32_t)h << 2);
@@ -176,9 +177,10 @@ template <typename F, typename R, int NR>
 __device__ __forceinline__ uint32_t hb_update_link_rt(const Geom& g, const F& f, int mu, int par, uint32_t i, R beta,
                                                       uint32_t k0, uint32_t k1, uint32_t sweep, int n_hits) {
   const Coord x = cb_coord(g, par, i);
+  if (!own_site(g, x.c[3])) return 0;  // halo slice of a slab
   const m3<R> A = staple_sum_rt<F, R>(g, f, x, mu, par, i);
   m3<R> U = f.template load<R>(mu, par, i);
-  const uint32_t link = (uint32_t)mu * g.V + x.s;
+  const uint32_t link = (uint32_t)mu * g.Vg + (x.s + g.soff);
   uint32_t fails = 0;
   for (int h = 0; h < n_hits; ++h) {
     const uint32_t hb = RNG_DOMAIN_HB | ((uint32_t)h << 2);

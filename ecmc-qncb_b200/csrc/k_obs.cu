@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(RED_THREADS, RedMinBlocks<S>::value) k_plaquet
     const int par = (int)(t & 1);
     const uint32_t i = (uint32_t)(t >> 1);
     const Coord x = cb_coord(g, par, i);
-    acc += (double)site_plaquette<Links<S, NR>, S>(g, f, x, par, i);
+    if (own_site(g, x.c[3])) acc += (double)site_plaquette<Links<S, NR>, S>(g, f, x, par, i);
   }
   double b = block_sum<RED_THREADS>(acc, sh);
   if (threadIdx.x == 0) parts[blockIdx.x] = b;
@@ -150,6 +150,7 @@ __global__ void __launch_bounds__(RED_THREADS, RedMinBlocks<S>::value) k_clover_
     const int par = (int)(t & 1);
     const uint32_t i = (uint32_t)(t >> 1);
     const Coord x = cb_coord(g, par, i);
+    if (!own_site(g, x.c[3])) continue;
     R q = 0, e = 0;
     site_qe<Links<S, NR>, R>(g, f, x, par, i, &q, &e);
     accq += (double)q;
@@ -177,7 +178,7 @@ static cudaError_t clover_impl(const LatDev& L, double* scratch, double* out2, c
   const int nb = red_grid(L.g);
   k_clover_qe<S, NR><<<nb, RED_THREADS, 0, s>>>(L.g, f, scratch);
   k_finalize<<<1, 64, 0, s>>>(scratch, nb, 2, out2);
-  k_qe_scale<<<1, 1, 0, s>>>(out2, 1.0 / (double)L.g.V);
+  k_qe_scale<<<1, 1, 0, s>>>(out2, 1.0 / (double)L.g.Vg);
   return cudaGetLastError();
 }
 

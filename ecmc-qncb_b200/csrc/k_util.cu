@@ -17,6 +17,21 @@ Geom make_geom(const int dims[4]) {
   g.stride = (g.Vh + 63u) & ~63u;
   const uint32_t dv[3] = {(uint32_t)g.Lxh, (uint32_t)dims[1], (uint32_t)dims[2]};
   for (int k = 0; k < 3; ++k) g.rcp[k] = dv[k] == 1 ? 0xFFFFFFFFu : (uint32_t)((1ull << 32) / dv[k]);
+  g.tlo = 0;
+  g.thi = dims[3] - 1;
+  g.Vg = g.V;
+  g.soff = 0;
+  return g;
+}
+
+Geom make_slab_geom(const int global_dims[4], int t0, int tl) {
+  const int local[4] = {global_dims[0], global_dims[1], global_dims[2], tl + 2};
+  Geom g = make_geom(local);
+  g.tlo = 1;
+  g.thi = tl;
+  g.Vg = (uint32_t)global_dims[0] * (uint32_t)global_dims[1] * (uint32_t)global_dims[2] * (uint32_t)global_dims[3];
+  // local time 1 is global time t0: global index = local index + (t0 - 1) str[3] (mod 2^32)
+  g.soff = (uint32_t)((int64_t)(t0 - 1) * (int64_t)g.str[3]);
   return g;
 }
 
@@ -99,7 +114,7 @@ __global__ void k_hot(Geom g, Links<S, NR> f, uint32_t k0, uint32_t k1) {
   for (int b = 0; b < 8; ++b) {
     const int mu = b >> 1, par = b & 1;
     const Coord x = cb_coord(g, par, i);
-    const uint32_t link = (uint32_t)mu * g.V + x.s;
+    const uint32_t link = (uint32_t)mu * g.Vg + global_site(g, x.s);
     f.template store<double>(mu, par, i, haar_su3(link, RNG_DOMAIN_HOT, k0, k1));
   }
 }

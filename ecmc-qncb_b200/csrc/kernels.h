@@ -23,6 +23,9 @@ struct AlgDev {
 size_t link_bytes(const Geom& g, int prec, int nr);
 size_t alg_bytes(const Geom& g, int prec);
 Geom make_geom(const int dims[4]);
+// Slab of global lattice global_dims: global times t0 .. t0 + tl - 1 as local times 1 .. tl,
+// plus one halo time slice on each side (local extents Lx, Ly, Lz, tl + 2).
+Geom make_slab_geom(const int global_dims[4], int t0, int tl);
 
 // ---- util (k_util.cu) --------------------------------------------------------------
 cudaError_t launch_cold(const LatDev& L, cudaStream_t s, int block);

@@ -31,7 +31,26 @@ struct Geom {
   uint32_t Vh;   // V / 2
   uint32_t stride;  // allocation stride of one chunk array (>= Vh, multiple of 64)
   uint32_t rcp[3];  // floor(2^32 / d) for d = Lxh, Ly, Lz (0xFFFFFFFF for d = 1)
+  // Slab of a larger lattice (domain decomposition along t): the sites with local time
+  // tlo .. thi are the slab's own, the slices outside are halo copies of the neighbours'.
+  // Random-number link ids and the normalisation of the observables use the global volume
+  // Vg and the global site index s + soff (mod 2^32).  A whole lattice has tlo = 0,
+  // thi = Lt - 1, Vg = V, soff = 0.
+  int tlo, thi;
+  uint32_t Vg;
+  uint32_t soff;
 };
+
+__device__ __forceinline__ bool own_site(const Geom& g, int t) { return t >= g.tlo && t <= g.thi; }
+
+// Global site index of local full index s, periodic in the global time (halo slices of the
+// first and last slab wrap around; volumes are below 2^30, so the signed view is exact).
+__device__ __forceinline__ uint32_t global_site(const Geom& g, uint32_t s) {
+  int32_t gs = (int32_t)(s + g.soff);
+  if (gs < 0) gs += (int32_t)g.Vg;
+  else if ((uint32_t)gs >= g.Vg) gs -= (int32_t)g.Vg;
+  return (uint32_t)gs;
+}
 
 // n / d and n % d by multiply-high with r = rcp of d: the estimate umulhi(n, r) is q or
 // q - 1 for every 32-bit n, so one correction step makes it exact.

@@ -468,6 +468,7 @@ int qcb_server_submit(qcb_server* s, const qcb_job* job, uint64_t* id) {
   if (!s || !job || !job->lat) return set_error(QCB_ERR_INVALID, "null argument");
   const qcb_lattice* L = job->lat;
   if (L->ctx != s->ctx) return set_error(QCB_ERR_INVALID, "job lattice belongs to another context");
+  if (L->slab_tl) return set_error(QCB_ERR_INVALID, "a slab cannot be served (it needs halo exchanges)");
   if (L->dev.prec != s->cfg.precision || L->dev.nr != s->cfg.storage)
     return set_error(QCB_ERR_INVALID, "job lattice precision/storage differs from the server's");
   if (job->kind == QCB_JOB_SWEEPS) {

@@ -132,6 +132,15 @@ SIGNATURES = {
     "qcb_server_clock": (C.c_double, [_vp]),
     "qcb_server_destroy": (C.c_int, [_vp]),
     "qcb_wait_selftest": (C.c_int, [_vp, C.c_double, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "qcb_lattice_create_slab": (C.c_int, [_vp, _ip, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "qcb_slab_info": (C.c_int, [_vp, _ip, _ip, _ip]),
+    "qcb_heatbath_pass": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_uint64, C.c_uint64]),
+    "qcb_flow_stage": (C.c_int, [_vp, C.c_int, C.c_double, C.c_int]),
+    "qcb_flow_finish": (C.c_int, [_vp, C.c_int]),
+    "qcb_slab_exchange": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_int]),
+    "qcb_slab_face": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p),
+                                C.POINTER(C.c_size_t), _ip]),
+    "qcb_slab_face_copy": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int]),
     "qcb_params_default": (C.c_int, [C.POINTER(HbParams)]),
     "qcb_params_load": (C.c_int, [C.c_char_p, C.POINTER(HbParams)]),
 }

@@ -216,6 +216,45 @@ int qcb_batch_run(qcb_batch* b, const qcb_batch_plan* plan, const double* betas,
  * NULL = no cache) under keys "<device name>|<precision>-<storage>|<hb|flow>|LxLyLzLt". */
 int qcb_batch_autotune(qcb_batch* b, const char* cache_path);
 
+/* ---- slabs: one lattice split along t over several devices or processes ------------------
+ * A slab holds global times t0 .. t0 + t_local - 1 of a lattice of extents global_dims as
+ * local times 1 .. t_local, plus one halo time slice on each side (local extents Lx, Ly, Lz,
+ * t_local + 2).  t0 and t_local must be even.  It replaces the reference's MPI block
+ * decomposition with halo exchange (src/mpi/HalosExchange.cpp, src/geometry/GeometryCB.cpp)
+ * by a decomposition along t with one face exchange per heatbath pass or flow stage.
+ * Random numbers are keyed by the global link, so N slabs reproduce the whole-lattice run
+ * bit for bit.  qcb_set_links / qcb_get_links use the local sites (halos included);
+ * qcb_plaquette and qcb_topo_qe return the slab's contribution to the global mean plaquette,
+ * Q and E (sum them over the slabs).  qcb_heatbath, qcb_heatbath_frozen, qcb_translate,
+ * qcb_flow_steps, qcb_flow_measure and the ILDG calls return QCB_ERR_STATE on a slab. */
+int qcb_lattice_create_slab(qcb_ctx* ctx, const int global_dims[4], int t0, int t_local, int precision,
+                            int storage, qcb_lattice** out);
+int qcb_slab_info(const qcb_lattice* lat, int global_dims[4], int* t0, int* t_local);
+/* One checkerboard heatbath pass (direction mu, global parity) of sweep `sweep`; on a
+ * whole lattice the same as one pass of qcb_heatbath. */
+int qcb_heatbath_pass(qcb_lattice* lat, int mu, int parity, double beta, int n_hits, uint64_t seed,
+                      uint64_t sweep);
+/* Stage 1, 2 or 3 of RK3 step `step` of the Wilson flow, in place as qcb_flow_steps: step s
+ * uses the links (a) and the lattice's work buffer (b), swapped for odd s; stage 1 writes b,
+ * stage 2 writes a, stage 3 writes b.  qcb_flow_finish(lat, n) after n steps moves the
+ * result into the links when n is odd. */
+int qcb_flow_stage(qcb_lattice* lat, int stage, double eps, int step);
+int qcb_flow_finish(qcb_lattice* lat, int n_steps);
+/* Face exchange between slab `lower` and the slab `upper` that follows it in time
+ * (periodically): lower's last own slice -> upper's low halo, upper's first own slice ->
+ * lower's high halo, for the links (which = 0) or the flow work buffer (which = 1), of
+ * direction mu (-1: all) and global parity (-1: both).  Waits for both slabs' streams;
+ * peer copies when the slabs are on different devices. */
+int qcb_slab_exchange(qcb_lattice* lower, qcb_lattice* upper, int which, int mu, int parity);
+/* Device pointers of one face, for an exchange by another transport (NCCL send / recv):
+ * side 0 low halo, 1 first own slice, 2 last own slice, 3 high halo; *n_segments contiguous
+ * segments of *bytes bytes each. */
+int qcb_slab_face(qcb_lattice* lat, int which, int side, int mu, int parity, void** segments, size_t* bytes,
+                  int* n_segments);
+/* Copies one face to (to_face = 0) or from (to_face = 1) a contiguous buffer of
+ * n_segments * bytes bytes, host or device memory; synchronous. */
+int qcb_slab_face_copy(qcb_lattice* lat, int which, int side, int mu, int parity, void* buf, int to_face);
+
 /* ---- failure detection --------------------------------------------------------------
  * The persistent batch and server kernels wait on per-lattice counters that other blocks
  * advance; every wait is bounded (2 s of wall-clock time or 2^28 polls), after which the

@@ -60,3 +60,18 @@ def test_single_process_is_a_no_op(monkeypatch):
         monkeypatch.delenv(k, raising=False)
     assert replicas.init("gloo") is None
     assert replicas.max_over_ranks(3.5) == 3.5
+
+
+def test_slab_split_and_flow_buffers():
+    from qcb import slabs
+
+    assert slabs._split((4, 4, 4, 16), 4) == [(0, 4), (4, 4), (8, 4), (12, 4)]
+    for bad in ((4, 4, 4, 12), 5), ((4, 4, 4, 12), 4):  # 12 / 5 not whole; 12 / 4 = 3 is odd
+        try:
+            slabs._split(*bad)
+            raise AssertionError("accepted a bad split")
+        except ValueError:
+            pass
+    # stage 1 and 3 write the work buffer on even steps, stage 2 the links; odd steps swap
+    assert [slabs.flow_dst(s, 0) for s in (1, 2, 3)] == [slabs.WORK, slabs.LINKS, slabs.WORK]
+    assert [slabs.flow_dst(s, 1) for s in (1, 2, 3)] == [slabs.LINKS, slabs.WORK, slabs.LINKS]
