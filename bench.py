@@ -302,6 +302,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         # throughput shows the latency of a server that keeps up.
         rate = 0.8 * result["serving"]["throughput_jobs_per_s"]
         result["serving_80pct_load"] = serving_section(ctx, n_requests=40, rate=rate)
+        result["plain"] = plain_section()
     return result
 
 
@@ -549,6 +550,72 @@ def large_workload(out_path=None) -> dict:
     if out_path:
         Path(out_path).write_text(json.dumps(out, indent=1) + "\n")
     return out
+
+
+# ---------------------------------------------------------------------------------------
+PLAIN_INPUT = """L_core=8
+n_core_dims=1
+cold_start=true
+seed=1234
+N_shift_therm = 0
+N_shift=200
+N_switch_eo=1
+beta = 6.0
+N_sweeps = 1
+N_hits = 1
+N_shift_plaquette = 1
+topo = false
+run_name = plain8
+run_dir = {run_dir}
+save_each_shifts = 1000
+"""
+
+
+def _plain_cpu(_):
+    """The plain-method workload with the reference schedule on one host core: 200 shifts of
+    one sweep with the plaquette each, then 50 RK3 flow steps (N_rk_steps = 1) with Q/E."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    t = time.perf_counter()
+    chain = oracle.RefChain(8, 1234, True)
+    chain.run(6.0, 200, 1, 1)
+    oracle.flow_measure(chain.links(), (8, 8, 8, 8), 0.02, 50, 1)
+    return time.perf_counter() - t
+
+
+def plain_section():
+    """Plain method (8^4, beta = 6.0, cold start, seed 1234, 200 sweeps with the plaquette each,
+    then the flow on the final configuration, eps = 0.02, 50 steps, FP64) end to end through the
+    drop-in driver gauge_hb_ncb (process start, parsing, device work, the output files), and
+    the same workload with the reference schedule on one host core (the oracle port)."""
+    import tempfile
+
+    driver = ROOT / "ecmc-qncb_b200" / "bin" / "gauge_hb_ncb"
+    with tempfile.TemporaryDirectory() as d:
+        inp = Path(d) / "in.txt"
+        inp.write_text(PLAIN_INPUT.format(run_dir=Path(d) / "data"))
+        t = time.perf_counter()
+        r = subprocess.run([str(driver), str(inp)], capture_output=True, text=True, timeout=600)
+        t_drv = time.perf_counter() - t
+        ok = r.returncode == 0
+        # the flow on the saved configuration, through the library (t = 0 .. 0.98)
+        import qcb
+
+        ctx = qcb.Context(0)
+        f = qcb.GaugeField(ctx, (8, 8, 8, 8))
+        f.load_ildg(Path(d) / "data" / "plain8" / "plain8")
+        t = time.perf_counter()
+        tqe = qcb.observables.topo_charge_flowed(f, qcb.GradientFlow(0.02), 50, 1)
+        t_flow = time.perf_counter() - t
+        f.close()
+        ctx.close()
+    with mp.get_context("spawn").Pool(1) as pool:
+        t_cpu = pool.map(_plain_cpu, [0])[0]
+    return {"workload": "8^4 beta=6.0 cold start seed 1234, 200 sweeps + plaquette each; flow eps=0.02, 50 steps",
+            "driver_ok": ok, "driver_wall_s": t_drv, "flow_wall_s": t_flow, "Q_final": float(tqe[-2]),
+            "cpu_reference_schedule_1core_s": t_cpu,
+            "note": "driver wall time includes process start, CUDA context creation and the output files"}
 
 
 # ---------------------------------------------------------------------------------------

@@ -143,6 +143,8 @@ struct Store<float, 12> {
 // Load path of a link read.  LD_RO: read-only data path (__ldg), for kernels that never
 // read links written earlier in the same launch.  LD_CG: L2-coherent loads (__ldcg), for
 // persistent kernels whose blocks read links other blocks wrote in the same launch.
+// (Ordinary L1-cached loads in the persistent kernels, after thread 0's acquire and a block
+// barrier, returned stale links: the batch-versus-single bit-identity test failed with them.)
 enum : int { LD_RO = 0, LD_CG = 1 };
 
 template <int LM, typename V>
@@ -266,7 +268,7 @@ struct AlgField {
     const S* q;
     V v[NC];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) v[c] = (LM == LD_RO) ? p[idx(mu, par, c, i)] : __ldcg(&p[idx(mu, par, c, i)]);
+    for (int c = 0; c < NC; ++c) v[c] = (LM == LD_CG) ? __ldcg(&p[idx(mu, par, c, i)]) : p[idx(mu, par, c, i)];
     q = reinterpret_cast<const S*>(v);
 #pragma unroll
     for (int k = 0; k < 8; ++k) z.a[k] = R(q[k]);
