@@ -6,8 +6,8 @@
 //   clover_site / local_q_e_clover / topo_q_e_clover(_global) (observables_mpi.cpp:61-150):
 //   F_{mu nu} = (C - C^dag)/8 with C the sum of the four leaves at x,
 //   q = (tr F01 F23 - tr F02 F13 + tr F03 F12) / (4 pi^2), e = 1/2 sum_{mu<nu} |F|^2.
-// Here: one thread per site (both parities), per-site value in the lattice's arithmetic
-// type, converted to FP64; FP64 tree reduction inside each block; the block partials are
+// Here: one thread per site (the two parities of a checkerboard index adjacent; a slab
+// skips its halo slices), per-site value in the lattice's arithmetic type, converted to FP64; FP64 tree reduction inside each block; the block partials are
 // summed in a fixed order with Neumaier compensation by a single-block kernel.  The grid
 // is a fixed multiple of the SM count (grid-stride loop), so the scratch is bounded.
 #include "dispatch.cuh"

@@ -4,9 +4,10 @@
 // free and the work-space arena (a single device allocation made at creation, the server's
 // HBM budget) has room for it, so later arrivals never overtake earlier ones.  Each tick
 // builds one descriptor per admitted job (a sweeps job advances by quantum_sweeps sweeps, a
-// flow job by quantum_steps RK3 steps, each lattice with its own level count), runs them in
-// one mixed persistent launch, measures the jobs that finished (batched plaquette / clover
-// reductions), copies the results back, and then admits the next arrivals.
+// flow job by quantum_steps RK3 steps, each lattice with its own level count), runs the
+// sweeps jobs in one persistent heatbath launch and the flow jobs in one persistent flow
+// launch, measures the jobs that finished (batched plaquette / clover reductions), copies the
+// results back, and then admits the next arrivals.
 #include <string.h>
 
 #include <chrono>
