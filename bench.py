@@ -58,6 +58,15 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def fp32_roof(units_per_s, flop_per_unit, peak_tflops):
+    """FP32 operation rate of a kernel from its ncu-counted operations per unit."""
+    if not flop_per_unit:
+        return None
+    achieved = units_per_s * flop_per_unit / 1e12
+    return {"achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s", "frac": achieved / peak_tflops,
+            "peak_kind": "nominal", "flop_per_unit": flop_per_unit}
+
+
 def ncu_traffic():
     """DRAM bytes per launch of the dominant kernels from the committed ncu summaries."""
     p = ROOT / "profiles" / "ncu_traffic.json"
@@ -204,6 +213,11 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     hb_achieved = hb_bytes_launch / (hb_pass_ms / 1e3) / 1e9
     flow_achieved = FLOW_BYTES[("fp32", 12)] * V / (rk3_ms / 1e3) / 1e9
     traffic = ncu_traffic()
+    # FP32 compute roofline beside the HBM one: ncu-counted FP32 operations per unit times
+    # the measured rate, against the nominal FP32 peak (148 SMs x 128 lanes x 2 x max clock;
+    # no FP32 peak is measured on this pool).
+    fp32_peak = 148 * 128 * 2 * float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get(
+        "sm_max_mhz", 1965.0)) * 1e6 / 1e12 if (ROOT / "MEASURED_PEAKS.json").exists() else 74.4
 
     # ---- FP64 path (same workload, one untimed-for-value step) ---------------------------
     f64 = qcb.GaugeField(ctx, dims, "fp64", 18)
@@ -278,14 +292,18 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                          "h2d_bytes_per_step": V * 72 * 8, "d2h_bytes_per_step": 3 * FLOW_RECORDS * 8},
                  "roofline": {"bound": "hbm", "achieved": flow_achieved, "peak": peak, "unit": "GB/s",
                               "frac": flow_achieved / peak, "peak_kind": peak_kind,
-                              "traffic": traffic.get("flow_stage_fp32r12_per_rk3")}},
+                              "traffic": traffic.get("flow_stage_fp32r12_per_rk3")},
+                 "fp32_compute": fp32_roof(V / (rk3_ms / 1e3), traffic.get("flow_fp32r12_fp32_flop_per_site_step"),
+                                           fp32_peak)},
         "fp64": {"hb_value": hb64_rate, "flow_value": flow64_rate, "storage": "fp64-18",
                  "hb_speedup_fp32": hb_rate / world / hb64_rate, "flow_speedup_fp32": flow_rate / world / flow64_rate},
         "precision": precision,
         "roofline": {"bound": "hbm", "kernel": "k_hb_pass<float,12>", "achieved": hb_achieved, "peak": peak,
                      "unit": "GB/s", "frac": hb_achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic.get("hb_pass_fp32r12_per_launch"),
-                     "algorithmic_bytes_per_launch": hb_bytes_launch, "launch_ms": hb_pass_ms},
+                     "algorithmic_bytes_per_launch": hb_bytes_launch, "launch_ms": hb_pass_ms,
+                     "fp32_compute": fp32_roof(V / 2 / (hb_pass_ms / 1e3),
+                                               traffic.get("hb_pass_fp32r12_fp32_flop_per_link_update"), fp32_peak)},
         "e2e": {"value": e2e_rate, "unit": "link-updates/s", "ms_per_step": e2e_hb_ms,
                 "h2d_bytes_per_step": V * 72 * 8, "d2h_bytes_per_step": 8,
                 "step": "qcb_set_links from pinned host FP64 links + 500 sweeps + plaquette to host"},
