@@ -287,11 +287,19 @@ int qcb_lattice_create(qcb_ctx* c, const int dims[4], int precision, int storage
   L->bytes = link_bytes(L->dev.g, precision, storage);
   if (cudaMalloc(&L->dev.links, L->bytes) != cudaSuccess) {
     cudaGetLastError();
+    const size_t bytes = L->bytes;
     delete L;
-    return fail(QCB_ERR_NOMEM, "cannot allocate " + std::to_string(L->bytes) + " bytes of link storage");
+    return fail(QCB_ERR_NOMEM, "cannot allocate " + std::to_string(bytes) + " bytes of link storage");
   }
-  CU(cudaMemsetAsync(L->dev.links, 0, L->bytes, c->stream), "memset");
-  CU(launch_cold(L->dev, c->stream, 0), "cold start");
+  {
+    cudaError_t e = cudaMemsetAsync(L->dev.links, 0, L->bytes, c->stream);
+    if (e == cudaSuccess) e = launch_cold(L->dev, c->stream, 0);
+    if (e != cudaSuccess) {
+      cudaFree(L->dev.links);
+      delete L;
+      return cuda_fail(e, "lattice initialisation");
+    }
+  }
   c->launches++;
   c->refs++;  // under the context lock
   *out = L;
@@ -322,11 +330,19 @@ int qcb_lattice_create_slab(qcb_ctx* c, const int global_dims[4], int t0, int t_
   L->bytes = link_bytes(L->dev.g, precision, storage);
   if (cudaMalloc(&L->dev.links, L->bytes) != cudaSuccess) {
     cudaGetLastError();
+    const size_t bytes = L->bytes;
     delete L;
-    return fail(QCB_ERR_NOMEM, "cannot allocate " + std::to_string(L->bytes) + " bytes of link storage");
+    return fail(QCB_ERR_NOMEM, "cannot allocate " + std::to_string(bytes) + " bytes of link storage");
   }
-  CU(cudaMemsetAsync(L->dev.links, 0, L->bytes, c->stream), "memset");
-  CU(launch_cold(L->dev, c->stream, 0), "cold start");
+  {
+    cudaError_t e = cudaMemsetAsync(L->dev.links, 0, L->bytes, c->stream);
+    if (e == cudaSuccess) e = launch_cold(L->dev, c->stream, 0);
+    if (e != cudaSuccess) {
+      cudaFree(L->dev.links);
+      delete L;
+      return cuda_fail(e, "lattice initialisation");
+    }
+  }
   c->launches++;
   c->refs++;
   *out = L;
