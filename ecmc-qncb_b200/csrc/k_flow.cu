@@ -24,13 +24,17 @@ namespace qcb {
 // turn (to reuse the chunk's links from L2): 1.48 / 1.71 / 1.54 ms, because the direction
 // changes every one or two waves of blocks and the four instantiations then compete for the
 // instruction cache.  The flow is bound by instruction issue, not by DRAM.
-// Resident blocks per SM in FP32 (the register bound): 5 (96 registers) measured 1.36 ms
-// per RK3 step on 32^4 FP32-12 against 1.74 ms with the compiler's own choice.
+// Resident blocks per SM (the register bound): FP32 5 (96 registers) measured 1.36 ms per RK3
+// step on 32^4 FP32-12 against 1.74 ms with the compiler's own choice; FP64 3 measured
+// 2.76 ms per step on 32^4 FP64-18 against 3.02 ms with the compiler's own choice or 2.
 #ifndef QCB_FLOW_MINB32
 #define QCB_FLOW_MINB32 5
 #endif
+#ifndef QCB_FLOW_MINB64
+#define QCB_FLOW_MINB64 3
+#endif
 template <typename S, int NR, int STAGE>
-__global__ void __launch_bounds__(128, sizeof(S) == 4 ? QCB_FLOW_MINB32 : 1) k_flow_stage(Geom g, Links<S, NR> src, Links<S, NR> dst, AlgField<S> acc,
+__global__ void __launch_bounds__(128, sizeof(S) == 4 ? QCB_FLOW_MINB32 : QCB_FLOW_MINB64) k_flow_stage(Geom g, Links<S, NR> src, Links<S, NR> dst, AlgField<S> acc,
                                                     S eps) {
   const int mu = blockIdx.y;
   const uint32_t i = (blockIdx.x >> 1) * blockDim.x + threadIdx.x;

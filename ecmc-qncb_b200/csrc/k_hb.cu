@@ -19,13 +19,16 @@
 namespace qcb {
 
 // Blocks of 128 threads.  Resident blocks per SM (the register bound): FP32 5 (96
-// registers, measured 2.6% faster than 4 on 32^4), FP64 4 (a tighter bound spills).
+// registers, measured 2.6% faster than 4 on 32^4), FP64 3 (2.6% faster than 4, 2 slower).
 #ifndef QCB_HB_MINB32
 #define QCB_HB_MINB32 5
 #endif
+#ifndef QCB_HB_MINB64
+#define QCB_HB_MINB64 3
+#endif
 template <typename S>
 struct HbMinBlocks {
-  static constexpr int value = sizeof(S) == 4 ? QCB_HB_MINB32 : 4;
+  static constexpr int value = sizeof(S) == 4 ? QCB_HB_MINB32 : QCB_HB_MINB64;
 };
 
 // Frozen links of the reference's block decomposition (src/geometry/GeometryCB.cpp:33-56)
