@@ -687,8 +687,9 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="run only warmup + steps of the workload (for ncu); print launch counts")
     ap.add_argument("--storage", choices=["fp32-12", "fp64-18"], default="fp32-12")
-    ap.add_argument("--workload", choices=["precision", "large"], default="precision",
-                    help="large: the 64^4 single-lattice workload, printed as its own JSON object")
+    ap.add_argument("--workload", choices=["precision", "large", "batch"], default="precision",
+                    help="large: the 64^4 single-lattice workload; batch: the 64-lattice batching workload "
+                         "alone; each printed as its own JSON object")
     ap.add_argument("--out", default=None, help="also write the large-workload JSON to this path")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -720,6 +721,18 @@ def main():
     if args.workload == "large":
         if rank == 0:
             print(json.dumps(large_workload(args.out)))
+        return 0
+    if args.workload == "batch":
+        if rank == 0:
+            import torch
+
+            import qcb
+            from qcb import _lib
+
+            ctx = qcb.Context(0)
+            stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+            print(json.dumps(batch_section(ctx, _lib.lib(), stream)))
+            ctx.close()
         return 0
     dist = replicas.init("nccl", timeout_s=300)
     if args.profile:
