@@ -1,0 +1,37 @@
+// ecmc.h — launchers of the event-chain Monte Carlo kernels (k_ecmc.cu), library-internal.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/qcb.h"
+
+namespace qcb {
+
+// Size of the set of SU(3) elements near the identity (sample_persistant's set,
+// src/ecmc/ecmc_mpi_cb.cpp:560): the identity and 5000 pairs (M, M^dagger).
+constexpr int ECMC_SET_SIZE = 10001;
+
+// One sample call of every chain.
+struct EcmcLaunch {
+  double2* links;        // FP64 array-of-structures copy: link (s, mu) = 9 double2 at (4 s + mu) * 9
+  const double2* set;    // ECMC_SET_SIZE matrices of 9 double2
+  qcb_ecmc_chain* chains;
+  uint32_t n_chains;
+  int L[4];              // lattice extents
+  int nb[4];             // blocks per direction (L[d] / l)
+  int cum[4];            // cumulative shift of the field's frame, in [0, L[d])
+  int l;                 // block edge (l_core)
+  double beta, theta_sample, theta_refresh_site, theta_refresh_R;
+  int poisson;
+  uint32_t k0, k1;       // Philox key (seed)
+  uint32_t* status;      // OR of the chains' status bits
+};
+
+// The call's set, drawn from Philox counters (j, call_lo, call_hi, set domain).
+cudaError_t launch_ecmc_set(double2* set, double epsilon, uint64_t seed, uint64_t call, cudaStream_t s);
+cudaError_t launch_ecmc_sample(const EcmcLaunch& a, cudaStream_t s, int block);
+// out[0..2] += the chains' events, lifts, same-site lifts; zeroes them with reset.
+cudaError_t launch_ecmc_counters(qcb_ecmc_chain* chains, uint32_t n, unsigned long long* out, int reset,
+                                 cudaStream_t s);
+
+}  // namespace qcb

@@ -1,0 +1,633 @@
+// k_ecmc.cu — event-chain Monte Carlo: every l_core^4 block runs its own persistent chain,
+// one thread per chain, all chains of the lattice in one launch.
+//
+// The reference runs one chain per MPI rank (mpi::ecmccb::sample_persistant,
+// src/ecmc/ecmc_mpi_cb.cpp:496-637) on a padded block whose halo and low faces are frozen
+// (src/geometry/GeometryCB.cpp:33-56).  Every link a chain reads outside its own active
+// links is frozen in the block that owns it, so no chain ever reads a link that another
+// chain writes, and the chains of all blocks can run at the same time.  Links are read and
+// written in an FP64 array-of-structures copy of the lattice (one link = 9 consecutive
+// double2, 144 contiguous bytes): a chain touches scattered links, and a contiguous link
+// costs 5 DRAM sectors where the structure-of-arrays layout costs 9.
+//
+// Random numbers: chain c's k-th uniform is Philox4x32-10 with counter (k_lo, k_hi, c,
+// ECMC_CHAIN) and key seed; the call's set of near-identity elements uses counters
+// (j, call_lo, call_hi, ECMC_SET).  The arithmetic follows the reference's order of
+// operations, so the CPU oracle (same counters) reproduces every event.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ecmc.h"
+#include "philox.cuh"
+#include "su3.cuh"
+
+namespace qcb {
+namespace {
+
+constexpr uint32_t ECMC_CHAIN = 0xECEC0001u, ECMC_SET = 0xECEC0002u;
+constexpr uint64_t ECMC_MAX_EVENTS = 1ull << 26;
+constexpr double PI = 3.141592653589793;  // the double nearest pi
+
+typedef m3<double> M;
+typedef cx<double> Z;
+
+// Uniform in (0, 1) from two 32-bit words: (top 53 bits of hi:lo + 1/2) 2^-53.
+__device__ __forceinline__ double u53(uint32_t lo, uint32_t hi) {
+  const uint64_t x = ((((uint64_t)hi) << 32) | lo) >> 11;
+  return ((double)x + 0.5) * 1.1102230246251565e-16;
+}
+
+struct Stream {
+  uint32_t chain, k0, k1;
+  uint64_t n;
+  __device__ __forceinline__ double uni() {
+    u32x4 c;
+    c.v[0] = (uint32_t)n;
+    c.v[1] = (uint32_t)(n >> 32);
+    c.v[2] = chain;
+    c.v[3] = ECMC_CHAIN;
+    ++n;
+    const u32x4 r = philox4x32_10(c, k0, k1);
+    return u53(r.v[0], r.v[1]);
+  }
+};
+
+// SU(3) from 12 standard normals: rows 0, 1 complex Gaussian, Gram-Schmidt, row 2 =
+// conj(row0 x row1) (Haar-distributed).
+__device__ M haar_from_normals(const double n[12]) {
+  Z r0[3], r1[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    r0[j] = mk(n[2 * j], n[2 * j + 1]);
+    r1[j] = mk(n[6 + 2 * j], n[6 + 2 * j + 1]);
+  }
+  const double s0 = sqrt(r0[0].re * r0[0].re + r0[0].im * r0[0].im + r0[1].re * r0[1].re + r0[1].im * r0[1].im +
+                         r0[2].re * r0[2].re + r0[2].im * r0[2].im);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) r0[j] = mk(r0[j].re / s0, r0[j].im / s0);
+  Z d = conj(r0[0]) * r1[0] + conj(r0[1]) * r1[1] + conj(r0[2]) * r1[2];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) r1[j] = r1[j] - d * r0[j];
+  const double s1 = sqrt(r1[0].re * r1[0].re + r1[0].im * r1[0].im + r1[1].re * r1[1].re + r1[1].im * r1[1].im +
+                         r1[2].re * r1[2].re + r1[2].im * r1[2].im);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) r1[j] = mk(r1[j].re / s1, r1[j].im / s1);
+  M u;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    u.e[0][j] = r0[j];
+    u.e[1][j] = r1[j];
+  }
+  u.e[2][0] = conj(r0[1] * r1[2] - r0[2] * r1[1]);
+  u.e[2][1] = conj(r0[2] * r1[0] - r0[0] * r1[2]);
+  u.e[2][2] = conj(r0[0] * r1[1] - r0[1] * r1[0]);
+  return u;
+}
+
+// random_su3 (src/su3/utils.cpp:13-30), redrawn: Haar SU(3) from 6 Box-Muller pairs.
+__device__ M haar(Stream& g) {
+  double n[12];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const double u1 = g.uni(), u2 = g.uni();
+    const double rad = sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincos(2 * PI * u2, &sn, &cs);
+    n[2 * k] = rad * cs;
+    n[2 * k + 1] = rad * sn;
+  }
+  return haar_from_normals(n);
+}
+
+__device__ __forceinline__ M ld(const double2* links, uint32_t s, int mu) {
+  const double2* q = links + ((size_t)s * 4 + (size_t)mu) * 9;
+  M u;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    const double2 v = q[c];
+    u.e[c / 3][c % 3] = mk(v.x, v.y);
+  }
+  return u;
+}
+
+__device__ __forceinline__ void st(double2* links, uint32_t s, int mu, const M& u) {
+  double2* q = links + ((size_t)s * 4 + (size_t)mu) * 9;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) q[c] = make_double2(u.e[c / 3][c % 3].re, u.e[c / 3][c % 3].im);
+}
+
+__device__ __forceinline__ M adj(const M& a) {
+  M r;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r.e[i][j] = conj(a.e[j][i]);
+  return r;
+}
+
+// The block of one chain: local coordinates lc (in [-1, l] for every link a chain at an
+// active link reads; -1 and l are the neighbouring blocks' faces, the reference's halo) sit
+// at stored site b_d l + lc_d - cum_d (mod L_d), with base_d = b_d l - cum_d in
+// (-L_d, L_d - l].
+struct Block {
+  int L[4], base[4], l;
+  __device__ __forceinline__ uint32_t site(const int lc[4]) const {
+    uint32_t s = 0;
+#pragma unroll
+    for (int d = 3; d >= 0; --d) {
+      int c = base[d] + lc[d];
+      if (c < 0) c += L[d];
+      else if (c >= L[d]) c -= L[d];
+      // a chain only leaves [-1, l] after a lift onto a frozen link, which takes a rounding
+      // accident in the lift's tower sampling; the full reduction keeps any position in bounds
+      if ((unsigned)c >= (unsigned)L[d]) c = ((c % L[d]) + L[d]) % L[d];
+      s = s * (uint32_t)L[d] + (uint32_t)c;
+    }
+    return s;
+  }
+  // GeometryCB::is_frozen in block-local terms: the halo (outside [0, l)) and the links
+  // leaving local coordinate 0 in a direction d != mu.
+  __device__ __forceinline__ bool frozen(const int lc[4], int mu) const {
+    bool f = false;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) f = f || lc[d] < 0 || lc[d] >= l || (d != mu && lc[d] == 0);
+    return f;
+  }
+};
+
+__device__ __forceinline__ void shifted(const int a[4], int d1, int s1, int d2, int s2, int out[4]) {
+#pragma unroll
+  for (int d = 0; d < 4; ++d) out[d] = a[d] + (d == d1 ? s1 : 0) + (d == d2 ? s2 : 0);
+}
+
+// solve_reject_fast (src/ecmc/ecmc_mpi_cb.h:59-94): along U(theta) = R diag(e^{i eps theta},
+// e^{-i eps theta}, 1) R^dagger U one staple's action is A cos(theta) + eps B sin(theta) +
+// const; the angle at which the integral of its derivative's positive part reaches gamma.
+__device__ double solve_reject(double A, double B, double gamma, int eps) {
+  if (eps == -1) B = -B;
+  const double R = hypot(A, B), invR = 1.0 / R, period = 2.0 * R;
+  const double disc = floor(gamma / period);
+  gamma -= disc * period;
+  double phi = atan2(-A, B);
+  if (phi < 0.0) phi += 2.0 * PI;
+  const double p1 = R - A;
+  double alpha;
+  if (phi < PI * 0.5 || phi > PI * 1.5)
+    alpha = (gamma > p1) ? (gamma - p1) * invR - 1.0 : (gamma + A) * invR;
+  else
+    alpha = gamma * invR - 1.0;
+  alpha = alpha > 1.0 ? 1.0 : (alpha < -1.0 ? -1.0 : alpha);
+  double theta = phi + asin(alpha);
+  if (theta < 0.0) theta += 2.0 * PI;
+  if (theta >= 2.0 * PI) theta -= 2.0 * PI;
+  return theta + 2.0 * PI * disc;
+}
+
+// compute_reject_angles_fast (ecmc_mpi_cb.cpp:197-246) for one staple S, T = R^dagger U:
+// P = T S R; A = -(beta/3) Re(P00 + P11), B = -(beta/3) Im(P11 - P00).  Only P00 and P11
+// are needed, so S is never formed: a forward staple is S = X W^+ (W = U_nu(x) U_mu(x+nu),
+// X = U_nu(x+mu)) and P_ii = (T_i. X) . (W^+ R)_.i; a backward staple is S = W^+ D
+// (W = U_mu(x-nu) U_nu(x+mu-nu), D = U_nu(x-nu)) and P_ii = (T_i. W^+) . (D R)_.i.
+__device__ __forceinline__ double reject_from(Z P00, Z P11, double beta, double gamma, int eps) {
+  const double br = -(beta / 3.0);
+  return solve_reject((P00.re + P11.re) * br, (P11.im - P00.im) * br, gamma, eps);
+}
+
+// compute_ds (ecmc_mpi_cb.cpp:263-274), Im[(R^dagger P R)_00 - (R^dagger P R)_11], as
+// Im tr(P Q) with the Hermitian Q = R diag(1, -1, 0) R^dagger formed once per lift.
+struct Herm {
+  double d[3];  // real diagonal
+  Z o[3];       // Q01, Q02, Q12 (Q10 = conj Q01, ...)
+};
+__device__ __forceinline__ Herm ds_matrix(const M& R) {
+  Herm q;
+#pragma unroll
+  for (int m = 0; m < 3; ++m)
+    q.d[m] = R.e[m][0].re * R.e[m][0].re + R.e[m][0].im * R.e[m][0].im - R.e[m][1].re * R.e[m][1].re -
+             R.e[m][1].im * R.e[m][1].im;
+  q.o[0] = R.e[0][0] * conj(R.e[1][0]) - R.e[0][1] * conj(R.e[1][1]);
+  q.o[1] = R.e[0][0] * conj(R.e[2][0]) - R.e[0][1] * conj(R.e[2][1]);
+  q.o[2] = R.e[1][0] * conj(R.e[2][0]) - R.e[1][1] * conj(R.e[2][1]);
+  return q;
+}
+// Im tr(P Q) = sum_km Im(P_km Q_mk)
+__device__ __forceinline__ double ds_of(const M& P, const Herm& q) {
+  double s = P.e[0][0].im * q.d[0] + P.e[1][1].im * q.d[1] + P.e[2][2].im * q.d[2];
+  // P_01 Q_10 + P_10 Q_01 with Q_10 = conj(Q_01), and likewise for (0,2), (1,2)
+  const int a[3] = {0, 0, 1}, b[3] = {1, 2, 2};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const Z pab = P.e[a[k]][b[k]], pba = P.e[b[k]][a[k]], o = q.o[k];
+    s += pab.re * (-o.im) + pab.im * o.re;  // Im(P_ab conj(o))
+    s += pba.re * o.im + pba.im * o.re;     // Im(P_ba o)
+  }
+  return s;
+}
+
+// dS of lift candidate i under Q (not inlined: keeps the lift's link loads and products out
+// of the event loop's register budget).
+__device__ __noinline__ double lift_ds(int i, bool fwd, const double2* L, uint32_t s0, uint32_t s1, uint32_t s2,
+                                       uint32_t s3, int mu, int nu, Herm q);
+
+__device__ __forceinline__ int dsign(double x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
+
+// Link i of lift plaquette (fwd, nu) at local coordinates out, direction returned
+// (GeometryCB.cpp:58-90): 0 = (x, mu); forward 1 = (x+mu, nu), 2 = (x+nu, mu), 3 = (x, nu);
+// backward 1 = (x+mu-nu, nu), 2 = (x-nu, mu), 3 = (x-nu, nu).
+__device__ __forceinline__ int lift_link(int i, bool fwd, const int lc[4], int mu, int nu, int out[4]) {
+  switch (i) {
+    case 0: shifted(lc, -1, 0, -1, 0, out); return mu;
+    case 1: shifted(lc, mu, 1, fwd ? -1 : nu, fwd ? 0 : -1, out); return nu;
+    case 2: shifted(lc, nu, fwd ? 1 : -1, -1, 0, out); return mu;
+    default: shifted(lc, fwd ? -1 : nu, fwd ? 0 : -1, -1, 0, out); return nu;
+  }
+}
+
+// The plaquette of lift candidate i, read from link i (lift_improved_fast,
+// ecmc_mpi_cb.cpp:293-316), links loaded where they are used: forward P0 = U0 U1 (U3 U2)^+,
+// P1 = U1 (U3 U2)^+ U0, P2 = U2 (U0 U1)^+ U3 (P3 = P0^+); backward T = U0 (U2 U1)^+,
+// P0 = T U3, P1 = U1 U0^+ U3^+ U2, P3 = U3 T (P2 = P3^+).  s0..s3 are the links' sites.
+__device__ __forceinline__ M lift_plaquette(int i, bool fwd, const double2* L, uint32_t s0, uint32_t s1, uint32_t s2,
+                                            uint32_t s3, int mu, int nu) {
+  if (fwd) {
+    if (i == 0) return mul_na(mul_nn(ld(L, s0, mu), ld(L, s1, nu)), mul_nn(ld(L, s3, nu), ld(L, s2, mu)));
+    if (i == 1) return mul_nn(mul_na(ld(L, s1, nu), mul_nn(ld(L, s3, nu), ld(L, s2, mu))), ld(L, s0, mu));
+    return mul_nn(mul_na(ld(L, s2, mu), mul_nn(ld(L, s0, mu), ld(L, s1, nu))), ld(L, s3, nu));
+  }
+  if (i == 1) return mul_nn(mul_na(mul_na(ld(L, s1, nu), ld(L, s0, mu)), ld(L, s3, nu)), ld(L, s2, mu));
+  const M Tb = mul_na(ld(L, s0, mu), mul_nn(ld(L, s2, mu), ld(L, s1, nu)));
+  if (i == 0) return mul_nn(Tb, ld(L, s3, nu));
+  return mul_nn(ld(L, s3, nu), Tb);
+}
+
+__device__ __noinline__ double lift_ds(int i, bool fwd, const double2* L, uint32_t s0, uint32_t s1, uint32_t s2,
+                                       uint32_t s3, int mu, int nu, Herm q) {
+  return ds_of(lift_plaquette(i, fwd, L, s0, s1, s2, s3, mu, nu), q);
+}
+
+// su2_quaternion_to_su3 (src/su3/utils.cpp:33-45) of (x0, x1, x2, x3) in subgroup (i, j).
+__device__ M embed(const double x[4], int i, int j) {
+  M X;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) X.e[a][b] = mk(0.0, 0.0);
+  const int k = 3 - i - j;
+  X.e[k][k] = mk(1.0, 0.0);
+  X.e[i][i] = mk(x[0], x[3]);
+  X.e[j][j] = mk(x[0], -x[3]);
+  X.e[i][j] = mk(x[2], x[1]);
+  X.e[j][i] = mk(-x[2], x[1]);
+  return X;
+}
+
+// ecmc_set / random_SU3_epsilon (src/su3/utils.cpp:66-127): thread p writes set[2p+1] =
+// the product of (sqrt(1 - eps^2), eps r/|r|) embedded in (0,1), (0,2), (1,2), r uniform in
+// (-1/2, 1/2)^3, and set[2p+2] = its adjoint; thread 0 also writes set[0] = 1.
+__global__ void k_ecmc_set(double2* set, double eps, uint32_t k0, uint32_t k1, uint32_t call_lo, uint32_t call_hi) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= (ECMC_SET_SIZE - 1) / 2) return;
+  M Mx;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) Mx.e[a][b] = mk(a == b ? 1.0 : 0.0, 0.0);
+  if (p == 0)
+    for (int c = 0; c < 9; ++c) set[c] = make_double2(c % 4 == 0 ? 1.0 : 0.0, 0.0);
+  const int sub[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    double r[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      u32x4 c;
+      c.v[0] = (uint32_t)(p * 9 + 3 * s + d);
+      c.v[1] = call_lo;
+      c.v[2] = call_hi;
+      c.v[3] = ECMC_SET;
+      const u32x4 w = philox4x32_10(c, k0, k1);
+      r[d] = u53(w.v[0], w.v[1]) - 0.5;
+    }
+    const double norm = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    const double x[4] = {sqrt(1 - eps * eps), eps * r[0] / norm, eps * r[1] / norm, eps * r[2] / norm};
+    Mx = mul_nn(Mx, embed(x, sub[s][0], sub[s][1]));
+  }
+  double2* q = set + (size_t)(2 * p + 1) * 9;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) q[c] = make_double2(Mx.e[c / 3][c % 3].re, Mx.e[c / 3][c % 3].im);
+  q += 9;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) q[c] = make_double2(Mx.e[c % 3][c / 3].re, -Mx.e[c % 3][c / 3].im);
+}
+
+// sample_persistant (ecmc_mpi_cb.cpp:496-637) for chain c: events until it has travelled
+// theta_sample; the chain record persists across calls.
+__global__ void __launch_bounds__(64) k_ecmc_sample(EcmcLaunch a) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.n_chains) return;
+  qcb_ecmc_chain& rec = a.chains[c];
+  Block blk;
+  blk.l = a.l;
+  {
+    uint32_t q = c;
+#pragma unroll
+    for (int d = 3; d >= 0; --d) {
+      const int b = (int)(q % (uint32_t)a.nb[d]);
+      q /= (uint32_t)a.nb[d];
+      blk.L[d] = a.L[d];
+      blk.base[d] = b * a.l - a.cum[d];
+    }
+  }
+  Stream g;
+  g.chain = c;
+  g.k0 = a.k0;
+  g.k1 = a.k1;
+  g.n = rec.draws;
+  const int l = a.l;
+  const double2* set = a.set;
+  double2* links = a.links;
+  int lc[4], mu, eps;
+  double th_site, th_R, tr_site, tr_R;
+  uint64_t events, lifts, revs = rec.revs;
+  int status = rec.status;
+  M R;
+  if (!rec.initialized) {
+    // random_site (ecmc_mpi_cb.cpp:359-367): local coordinates 1 .. l-2 (padded 2 .. L-1)
+#pragma unroll
+    for (int d = 0; d < 4; ++d) lc[d] = 1 + (int)(g.uni() * (double)(l - 2));
+    mu = (int)(g.uni() * 4.0);
+    eps = g.uni() < 0.5 ? -1 : 1;
+    R = haar(g);
+    th_site = a.poisson ? -log(g.uni()) * a.theta_refresh_site : a.theta_refresh_site;
+    th_R = a.poisson ? -log(g.uni()) * a.theta_refresh_R : a.theta_refresh_R;
+    tr_site = tr_R = 0.0;
+    events = lifts = 0;
+  } else {
+#pragma unroll
+    for (int d = 0; d < 4; ++d) lc[d] = rec.site[d];
+    mu = rec.mu;
+    eps = rec.epsilon;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) R.e[k / 3][k % 3] = mk(rec.R[2 * k], rec.R[2 * k + 1]);
+    th_site = rec.theta_refresh_site;
+    th_R = rec.theta_refresh_R;
+    tr_site = rec.travelled_site;
+    tr_R = rec.travelled_R;
+    events = rec.events;
+    lifts = rec.lifts;
+  }
+  const double theta_sample = a.poisson ? -log(g.uni()) * a.theta_sample : a.theta_sample;
+  double tr_sample = 0.0;
+
+#pragma unroll 1
+  for (uint64_t ev = 0;; ++ev) {
+    if (ev >= ECMC_MAX_EVENTS) {
+      status |= 2;
+      break;
+    }
+    const uint32_t x = blk.site(lc);
+    // rows 0 and 1 of T = R^dagger U: all the reject angles need
+    M T;
+    {
+      const M U = ld(links, x, mu);
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j2 = 0; j2 < 3; ++j2)
+          T.e[i][j2] = conj(R.e[0][i]) * U.e[0][j2] + conj(R.e[1][i]) * U.e[1][j2] + conj(R.e[2][i]) * U.e[2][j2];
+    }
+    // compute_list_staples (ecmc_mpi_cb.cpp:12-36): for each nu != mu, forward then backward;
+    // the first minimum of the six reject angles
+    double best = 0.0;
+    int j = 0;
+#pragma unroll 1
+    for (int k = 0; k < 6; ++k) {
+      const int nu = (k >> 1) + ((k >> 1) >= mu ? 1 : 0);
+      int p[4], q[4];
+      Z P00 = mk(0.0, 0.0), P11 = mk(0.0, 0.0);
+      if ((k & 1) == 0) {  // U_nu(x+mu) (U_nu(x) U_mu(x+nu))^+
+        shifted(lc, mu, 1, -1, 0, p);
+        shifted(lc, nu, 1, -1, 0, q);
+        const M W = mul_nn(ld(links, x, nu), ld(links, blk.site(q), mu));
+        Z v0[3], v1[3];
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk) {
+          v0[kk] = conj(W.e[0][kk]) * R.e[0][0] + conj(W.e[1][kk]) * R.e[1][0] + conj(W.e[2][kk]) * R.e[2][0];
+          v1[kk] = conj(W.e[0][kk]) * R.e[0][1] + conj(W.e[1][kk]) * R.e[1][1] + conj(W.e[2][kk]) * R.e[2][1];
+        }
+        const M X = ld(links, blk.site(p), nu);
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk) {
+          P00 = P00 + (T.e[0][0] * X.e[0][kk] + T.e[0][1] * X.e[1][kk] + T.e[0][2] * X.e[2][kk]) * v0[kk];
+          P11 = P11 + (T.e[1][0] * X.e[0][kk] + T.e[1][1] * X.e[1][kk] + T.e[1][2] * X.e[2][kk]) * v1[kk];
+        }
+      } else {  // (U_mu(x-nu) U_nu(x+mu-nu))^+ U_nu(x-nu)
+        shifted(lc, mu, 1, nu, -1, p);
+        shifted(lc, nu, -1, -1, 0, q);
+        const uint32_t sq = blk.site(q);
+        const M W = mul_nn(ld(links, sq, mu), ld(links, blk.site(p), nu));
+        Z y0[3], y1[3];
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk) {
+          y0[kk] = T.e[0][0] * conj(W.e[kk][0]) + T.e[0][1] * conj(W.e[kk][1]) + T.e[0][2] * conj(W.e[kk][2]);
+          y1[kk] = T.e[1][0] * conj(W.e[kk][0]) + T.e[1][1] * conj(W.e[kk][1]) + T.e[1][2] * conj(W.e[kk][2]);
+        }
+        const M D = ld(links, sq, nu);
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk) {
+          P00 = P00 + y0[kk] * (D.e[kk][0] * R.e[0][0] + D.e[kk][1] * R.e[1][0] + D.e[kk][2] * R.e[2][0]);
+          P11 = P11 + y1[kk] * (D.e[kk][0] * R.e[0][1] + D.e[kk][1] * R.e[1][1] + D.e[kk][2] * R.e[2][1]);
+        }
+      }
+      const double rej = reject_from(P00, P11, a.beta, -log(g.uni()), eps);
+      if (k == 0 || rej < best) best = rej, j = k;
+    }
+    const double d_sample = theta_sample - tr_sample;
+    const double d_site = th_site - tr_site;
+    const double d_R = th_R - tr_R;
+    // std::min({...}) returns the first smallest; a non-finite step stops the chain
+    double step = best;
+    if (d_sample < step) step = d_sample;
+    if (d_site < step) step = d_site;
+    if (d_R < step) step = d_R;
+    if (!isfinite(step)) {
+      status |= 1;
+      break;
+    }
+    const int kind = (step == d_sample) ? 0 : (step == d_site) ? 1 : (step == d_R) ? 2 : 3;
+    // update (ecmc_mpi_cb.cpp:340-356): U <- R diag(e^{i xi}, e^{-i xi}, 1) R^dagger U
+    {
+      double sn, cs;
+      sincos((double)eps * step, &sn, &cs);
+      const M U = ld(links, x, mu);
+      M T2 = mul_an(R, U);
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        T2.e[0][cc] = T2.e[0][cc] * mk(cs, sn);
+        T2.e[1][cc] = T2.e[1][cc] * mk(cs, -sn);
+      }
+      st(links, x, mu, mul_nn(R, T2));
+      ++events;
+    }
+    if (kind == 0) {
+      tr_site += d_sample;
+      tr_R += d_sample;
+      break;
+    } else if (kind == 1) {
+      tr_sample += d_site;
+      tr_R += d_site;
+      tr_site = 0.0;
+      if (a.poisson) th_site = -log(g.uni()) * a.theta_refresh_site;
+#pragma unroll
+      for (int d = 0; d < 4; ++d) lc[d] = 1 + (int)(g.uni() * (double)(l - 2));
+      mu = (int)(g.uni() * 4.0);
+      eps = g.uni() < 0.5 ? -1 : 1;
+    } else if (kind == 2) {
+      tr_sample += d_R;
+      tr_site += d_R;
+      tr_R = 0.0;
+      if (a.poisson) th_R = -log(g.uni()) * a.theta_refresh_R;
+      R = haar(g);
+    } else {
+      tr_sample += best;
+      tr_site += best;
+      tr_R += best;
+      // lift_improved_fast (ecmc_mpi_cb.cpp:277-337) on plaquette j
+      const int nu = (j >> 1) + ((j >> 1) >= mu ? 1 : 0);
+      const bool fwd = (j & 1) == 0;
+      int t4[4];
+      lift_link(1, fwd, lc, mu, nu, t4);
+      const uint32_t s1 = blk.site(t4);
+      const bool f1 = blk.frozen(t4, nu);
+      lift_link(2, fwd, lc, mu, nu, t4);
+      const uint32_t s2 = blk.site(t4);
+      const bool f2 = blk.frozen(t4, mu);
+      lift_link(3, fwd, lc, mu, nu, t4);
+      const uint32_t s3 = blk.site(t4);
+      const bool f3 = blk.frozen(t4, nu);
+      const Herm Q = ds_matrix(R);
+      // dS of each candidate (0 for frozen links); the adjoint pair of the plaquette (forward
+      // 0 and 3, backward 2 and 3) has opposite dS
+      double ds0, ds1, ds2, ds3;
+      if (fwd) {
+        ds0 = lift_ds(0, true, links, x, s1, s2, s3, mu, nu, Q);
+        ds1 = f1 ? 0.0 : lift_ds(1, true, links, x, s1, s2, s3, mu, nu, Q);
+        ds2 = f2 ? 0.0 : lift_ds(2, true, links, x, s1, s2, s3, mu, nu, Q);
+        ds3 = f3 ? 0.0 : -ds0;
+      } else {
+        ds0 = lift_ds(0, false, links, x, s1, s2, s3, mu, nu, Q);
+        ds1 = f1 ? 0.0 : lift_ds(1, false, links, x, s1, s2, s3, mu, nu, Q);
+        const double d3 = lift_ds(3, false, links, x, s1, s2, s3, mu, nu, Q);
+        ds3 = f3 ? 0.0 : d3;
+        ds2 = f2 ? 0.0 : -d3;
+      }
+      const double a0 = fabs(ds0), a1 = fabs(ds1), a2 = fabs(ds2), a3 = fabs(ds3);
+      const double sum = a0 + a1 + a2 + a3;
+      const double p0 = a0 / sum, p1 = a1 / sum, p2 = a2 / sum;
+      // selectVariable (ecmc_mpi_cb.cpp:252-260)
+      const double r = g.uni();
+      const int idx = r < p0 ? 0 : (r < p0 + p1 ? 1 : (r < p0 + p1 + p2 ? 2 : 3));
+      const double ds_old = idx == 0 ? ds0 : idx == 1 ? ds1 : idx == 2 ? ds2 : ds3;
+      const int iset = (int)(g.uni() * (double)ECMC_SET_SIZE);
+      M Rn;
+      {
+        M Sx;
+        const double2* q = set + (size_t)iset * 9;
+#pragma unroll
+        for (int cc = 0; cc < 9; ++cc) {
+          const double2 v = q[cc];
+          Sx.e[cc / 3][cc % 3] = mk(v.x, v.y);
+        }
+        Rn = mul_nn(Sx, R);
+      }
+      // P of the chosen link: the adjoint partner reuses its pair's plaquette
+      double ds_new;
+      if (fwd && idx == 3)
+        ds_new = -lift_ds(0, true, links, x, s1, s2, s3, mu, nu, ds_matrix(Rn));
+      else if (!fwd && idx == 2)
+        ds_new = -lift_ds(3, false, links, x, s1, s2, s3, mu, nu, ds_matrix(Rn));
+      else
+        ds_new = lift_ds(idx, fwd, links, x, s1, s2, s3, mu, nu, ds_matrix(Rn));
+      int new_eps = -dsign(ds_old);
+      bool take = fabs(ds_old) < fabs(ds_new);
+      if (!take) take = g.uni() < fabs(ds_new) / fabs(ds_old);
+      if (take) {
+        R = Rn;
+        new_eps = -dsign(ds_new);
+      }
+      const int nmu = lift_link(idx, fwd, lc, mu, nu, t4);
+      const bool same = t4[0] == lc[0] && t4[1] == lc[1] && t4[2] == lc[2] && t4[3] == lc[3];
+      revs += same ? 1 : 0;
+      ++lifts;
+#pragma unroll
+      for (int d = 0; d < 4; ++d) lc[d] = t4[d];
+      mu = nmu;
+      eps = new_eps;
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 4; ++d) rec.site[d] = lc[d];
+  rec.mu = mu;
+  rec.epsilon = eps;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    rec.R[2 * k] = R.e[k / 3][k % 3].re;
+    rec.R[2 * k + 1] = R.e[k / 3][k % 3].im;
+  }
+  rec.theta_refresh_site = th_site;
+  rec.theta_refresh_R = th_R;
+  rec.travelled_site = tr_site;
+  rec.travelled_R = tr_R;
+  rec.draws = g.n;
+  rec.events = events;
+  rec.lifts = lifts;
+  rec.revs = revs;
+  rec.initialized = 1;
+  rec.status = status;
+  if (status) atomicOr(a.status, (uint32_t)status);
+}
+
+__global__ void k_ecmc_counters(qcb_ecmc_chain* chains, uint32_t n, unsigned long long* out, int reset) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long e = 0, l = 0, r = 0;
+  if (c < n) {
+    e = chains[c].events;
+    l = chains[c].lifts;
+    r = chains[c].revs;
+    if (reset) chains[c].events = chains[c].lifts = chains[c].revs = 0;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    e += __shfl_down_sync(0xffffffffu, e, o);
+    l += __shfl_down_sync(0xffffffffu, l, o);
+    r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  if ((threadIdx.x & 31) == 0 && (e | l | r)) {
+    atomicAdd(&out[0], e);
+    atomicAdd(&out[1], l);
+    atomicAdd(&out[2], r);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_ecmc_set(double2* set, double epsilon, uint64_t seed, uint64_t call, cudaStream_t s) {
+  const int pairs = (ECMC_SET_SIZE - 1) / 2;
+  k_ecmc_set<<<(pairs + 127) / 128, 128, 0, s>>>(set, epsilon, (uint32_t)seed, (uint32_t)(seed >> 32),
+                                                 (uint32_t)call, (uint32_t)(call >> 32));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ecmc_sample(const EcmcLaunch& a, cudaStream_t s, int block) {
+  if (block <= 0 || block > 64) block = 64;
+  k_ecmc_sample<<<(a.n_chains + block - 1) / block, block, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ecmc_counters(qcb_ecmc_chain* chains, uint32_t n, unsigned long long* out, int reset,
+                                 cudaStream_t s) {
+  k_ecmc_counters<<<(n + 127) / 128, 128, 0, s>>>(chains, n, out, reset);
+  return cudaGetLastError();
+}
+
+}  // namespace qcb

@@ -35,6 +35,7 @@ from ._lib import (FP32, FP64, R12, R18, BatchPlan, HbParams, Job, JobResult, Qc
                    check, lib)
 
 __all__ = ["Context", "GaugeField", "Batch", "BatchPlan", "Server", "PhiloxStream", "GradientFlow", "HbParams", "QcbError", "heatbathcb",
+           "EventChains", "EcmcParams", "ecmccb",
            "observables", "io", "save_ildg_clime", "read_ildg_clime", "FP32", "FP64", "R12", "R18",
            "device_count"]
 
@@ -424,3 +425,7 @@ class io:
         off, n = C.c_uint64(), C.c_uint64()
         check(lib().qcb_ildg_probe(os.fsencode(path), C.byref(off), C.byref(n)))
         return off.value, n.value
+
+
+from ._lib import EcmcParams  # noqa: E402
+from .ecmc import CHAIN_DTYPE, EventChains, ecmccb  # noqa: E402

@@ -76,6 +76,13 @@ class HbParams(C.Structure):
         return d
 
 
+class EcmcParams(C.Structure):
+    """qcb_ecmc_params: ECMCParams of the reference (src/io/params.h:9-17) plus the block edge."""
+    _fields_ = [("beta", C.c_double), ("theta_sample", C.c_double), ("theta_refresh_site", C.c_double),
+                ("theta_refresh_R", C.c_double), ("epsilon_set", C.c_double), ("poisson", C.c_int),
+                ("l_core", C.c_int)]
+
+
 _lib = None
 
 # name -> (restype, argtypes)
@@ -141,6 +148,13 @@ SIGNATURES = {
     "qcb_slab_face": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p),
                                 C.POINTER(C.c_size_t), _ip]),
     "qcb_slab_face_copy": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int]),
+    "qcb_ecmc_create": (C.c_int, [_vp, C.POINTER(EcmcParams), C.c_uint64, C.POINTER(C.c_void_p)]),
+    "qcb_ecmc_destroy": (C.c_int, [_vp]),
+    "qcb_ecmc_num_chains": (C.c_int, [_vp, _ip]),
+    "qcb_ecmc_sample": (C.c_int, [_vp, _ip]),
+    "qcb_ecmc_counters": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int]),
+    "qcb_ecmc_get_chains": (C.c_int, [_vp, _vp, C.POINTER(C.c_uint64)]),
+    "qcb_ecmc_set_chains": (C.c_int, [_vp, _vp, C.c_uint64]),
     "qcb_params_default": (C.c_int, [C.POINTER(HbParams)]),
     "qcb_params_load": (C.c_int, [C.c_char_p, C.POINTER(HbParams)]),
 }

@@ -323,6 +323,58 @@ int qcb_server_stats_get(qcb_server* s, qcb_server_stats* st);
 double qcb_server_clock(qcb_server* s);
 int qcb_server_destroy(qcb_server* s);
 
+/* ---- event-chain Monte Carlo ------------------------------------------------------------
+ * mpi::ecmccb::sample_persistant (src/ecmc/ecmc_mpi_cb.cpp:496-637) driven by
+ * generate_ecmc_cb (src/bin/gauge_ecmc_ncb.cpp:20-269).  The lattice is cut into blocks of
+ * edge l_core (one per MPI rank in the reference) and every block runs its own persistent
+ * event chain, all chains at once: one sample call moves every chain until it has travelled
+ * theta_sample (lifts, site refreshes and R refreshes as in the reference).  The blocks are
+ * placed as in qcb_heatbath_frozen: after the cumulative shift `shift` of the field's random
+ * translations, links with (x_d + shift_d) % l_core == 0 for some d != mu are frozen and
+ * block (bx, by, bz, bt) starts at x_d = b_d l_core - shift_d; its chain keeps its
+ * block-local position across calls.  Chain c = ((bx nby + by) nbz + bz) nbt + bt (the MPI
+ * Cartesian rank order) draws from Philox4x32-10 keyed by seed with counter (draw, c); the
+ * set of 10001 SU(3) elements near the identity (ecmc_set, src/su3/utils.cpp:119-127) is
+ * drawn once per call and shared by the chains.  The links are updated in FP64 whatever the
+ * lattice's storage.  The lattice is borrowed and must outlive the object. */
+typedef struct qcb_ecmc qcb_ecmc;
+typedef struct qcb_ecmc_params {
+  double beta;
+  double theta_sample;        /* param_theta_sample: angle travelled per sample call */
+  double theta_refresh_site;  /* param_theta_refresh_site */
+  double theta_refresh_R;     /* param_theta_refresh_R */
+  double epsilon_set;         /* epsilon_set: spread of the set around the identity, in [0, 1] */
+  int poisson;                /* budgets drawn from exponentials of these means */
+  int l_core;                 /* block edge, >= 3, dividing every extent */
+} qcb_ecmc_params;
+/* One chain (LocalChainState, src/ecmc/ecmc_mpi_cb.h:15-35), 256 bytes. */
+typedef struct qcb_ecmc_chain {
+  double R[18];               /* row-major 3x3 of (re, im) */
+  double theta_refresh_site, theta_refresh_R;   /* current budgets */
+  double travelled_site, travelled_R;           /* angle travelled since the last refreshes */
+  uint64_t draws;             /* position in the chain's Philox stream */
+  uint64_t events, lifts, revs;                 /* event, lift and same-site-lift counters */
+  int32_t site[4];            /* block-local x, y, z, t of the active link, in [0, l_core) */
+  int32_t mu, epsilon;        /* direction of the active link, sense of rotation (+1 / -1) */
+  int32_t initialized;        /* 0: drawn at the next call (site, mu, epsilon, R, budgets) */
+  int32_t status;             /* bit 0: non-finite event angle; bit 1: 2^26 events in one call */
+  int32_t pad[4];
+} qcb_ecmc_chain;
+int qcb_ecmc_create(qcb_lattice* lat, const qcb_ecmc_params* params, uint64_t seed, qcb_ecmc** out);
+int qcb_ecmc_destroy(qcb_ecmc* e);
+int qcb_ecmc_num_chains(const qcb_ecmc* e, int* n);
+/* One sample call of every chain (asynchronous).  shift = cumulative shift of the field. */
+int qcb_ecmc_sample(qcb_ecmc* e, const int shift[4]);
+/* Waits, then sums the chains' events, lifts and same-site lifts into out[0..2]; with reset,
+ * zeroes the three counters afterwards (the reference resets them after each plaquette
+ * measurement).  A chain that stopped on a non-finite angle or the event cap returns
+ * QCB_ERR_STATE (its bits are cleared). */
+int qcb_ecmc_counters(qcb_ecmc* e, uint64_t out[3], int reset);
+/* Copies the chain records (qcb_ecmc_num_chains of them) and the number of sample calls
+ * made so far (the key of the next call's set) to / from host memory; synchronous. */
+int qcb_ecmc_get_chains(qcb_ecmc* e, qcb_ecmc_chain* chains, uint64_t* calls);
+int qcb_ecmc_set_chains(qcb_ecmc* e, const qcb_ecmc_chain* chains, uint64_t calls);
+
 /* ---- input file ----------------------------------------------------------------------
  * io::load_params(..., RunParamsHbCB&) (src/io/io.cpp:353-399) with the defaults of
  * src/io/params.h:46-63.  Host-only.  Strings are NUL-terminated and truncated to fit. */

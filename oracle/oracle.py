@@ -62,6 +62,10 @@ def lib():
         L.orc_ref_sweeps.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int]
         L.orc_ref_get_links.argtypes = [C.c_void_p, dp]
         L.orc_ref_set_links.argtypes = [C.c_void_p, dp]
+        L.orc_ecmc_solve_reject.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, dp]
+        L.orc_ecmc_compute_ds.argtypes = [dp, dp, dp]
+        L.orc_ecmc_set.argtypes = [C.c_double, C.c_uint64, C.c_uint64, dp]
+        L.orc_ecmc_sample.argtypes = [dp, ip, dp, ip, C.c_uint64, C.c_uint64, ip, C.c_void_p]
         _lib = L
     return _lib
 
@@ -338,3 +342,57 @@ def load_params(path) -> dict:
         if k in cfg:
             p[k] = cfg[k]
     return p
+
+
+# ---- event-chain Monte Carlo (library form of mpi::ecmccb::sample_persistant) ------------
+# One record per chain, the layout of qcb_ecmc_chain in include/qcb.h (256 bytes).
+ECMC_CHAIN_DTYPE = np.dtype([
+    ("R", np.complex128, (3, 3)),
+    ("theta_refresh_site", np.float64), ("theta_refresh_R", np.float64),
+    ("travelled_site", np.float64), ("travelled_R", np.float64),
+    ("draws", np.uint64), ("events", np.uint64), ("lifts", np.uint64), ("revs", np.uint64),
+    ("site", np.int32, (4,)), ("mu", np.int32), ("epsilon", np.int32),
+    ("initialized", np.int32), ("status", np.int32), ("pad", np.int32, (4,)),
+])
+assert ECMC_CHAIN_DTYPE.itemsize == 256
+ECMC_SET_SIZE = 10001
+
+
+def ecmc_solve_reject(A, B, gamma, eps) -> float:
+    out = C.c_double()
+    lib().orc_ecmc_solve_reject(A, B, gamma, int(eps), C.byref(out))
+    return out.value
+
+
+def ecmc_compute_ds(P, R) -> float:
+    P = np.ascontiguousarray(P, np.complex128)
+    R = np.ascontiguousarray(R, np.complex128)
+    out = C.c_double()
+    lib().orc_ecmc_compute_ds(_dp(P), _dp(R), C.byref(out))
+    return out.value
+
+
+def ecmc_set(epsilon, seed, call) -> np.ndarray:
+    out = np.zeros((ECMC_SET_SIZE, 3, 3), np.complex128)
+    lib().orc_ecmc_set(epsilon, C.c_uint64(seed), C.c_uint64(call), _dp(out))
+    return out
+
+
+def ecmc_chains(dims, l_core) -> np.ndarray:
+    """Fresh (uninitialised) chain records, one per l_core^4 block."""
+    n = int(np.prod([d // l_core for d in dims]))
+    return np.zeros(n, ECMC_CHAIN_DTYPE)
+
+
+def ecmc_sample(u, dims, params: dict, seed, call, cum, chains):
+    """One sample call of every chain on a copy of u; returns (links, chains)."""
+    u = np.array(u, np.complex128, copy=True)
+    ch = np.array(chains, ECMC_CHAIN_DTYPE, copy=True)
+    dp = np.array([params["beta"], params["theta_sample"], params["theta_refresh_site"],
+                   params["theta_refresh_R"], params["epsilon_set"]], np.float64)
+    ip = (C.c_int * 2)(int(params.get("poisson", 0)), int(params["l_core"]))
+    rc = lib().orc_ecmc_sample(_dp(u), _dims(dims), _dp(dp), ip, C.c_uint64(seed), C.c_uint64(call),
+                               (C.c_int * 4)(*[int(c) for c in cum]), ch.ctypes.data_as(C.c_void_p))
+    if rc:
+        raise ValueError("l_core must be >= 3 and divide every extent")
+    return u, ch

@@ -20,6 +20,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
+#include <cmath>
 #include <complex>
 #include <limits>
 #include <random>
@@ -512,19 +514,9 @@ static uint64_t heatbath_cb(Lat& f, double beta, int n_sweeps, int n_hits, uint6
   return fails;
 }
 
-// Haar SU(3) from the Philox stream: rows 0, 1 complex Gaussian (Box-Muller), Gram-Schmidt,
-// row 2 = conj(row0 x row1).
-static M3 haar_philox(uint32_t id, uint32_t tag, uint32_t k0, uint32_t k1) {
-  double n[12];
-  for (int call = 0; call < 3; ++call) {
-    P4 r = philox({{id, 0u, tag, (uint32_t)call}}, k0, k1);
-    for (int pr = 0; pr < 2; ++pr) {
-      double u1 = u01(r.v[2 * pr]), u2 = u01(r.v[2 * pr + 1]);
-      double rad = sqrt(-2.0 * log(u1));
-      n[call * 4 + pr * 2 + 0] = rad * cos(2 * M_PI * u2);
-      n[call * 4 + pr * 2 + 1] = rad * sin(2 * M_PI * u2);
-    }
-  }
+// SU(3) matrix from 12 standard normals: rows 0, 1 complex Gaussian, Gram-Schmidt,
+// row 2 = conj(row0 x row1) (Haar-distributed).
+static M3 haar_from_normals(const double n[12]) {
   C r0[3], r1[3];
   for (int j = 0; j < 3; ++j) {
     r0[j] = C(n[2 * j], n[2 * j + 1]);
@@ -547,6 +539,21 @@ static M3 haar_philox(uint32_t id, uint32_t tag, uint32_t k0, uint32_t k1) {
   return u;
 }
 
+// Haar SU(3) from the Philox stream: 12 normals by Box-Muller from counters (id, 0, tag, call).
+static M3 haar_philox(uint32_t id, uint32_t tag, uint32_t k0, uint32_t k1) {
+  double n[12];
+  for (int call = 0; call < 3; ++call) {
+    P4 r = philox({{id, 0u, tag, (uint32_t)call}}, k0, k1);
+    for (int pr = 0; pr < 2; ++pr) {
+      double u1 = u01(r.v[2 * pr]), u2 = u01(r.v[2 * pr + 1]);
+      double rad = sqrt(-2.0 * log(u1));
+      n[call * 4 + pr * 2 + 0] = rad * cos(2 * M_PI * u2);
+      n[call * 4 + pr * 2 + 1] = rad * sin(2 * M_PI * u2);
+    }
+  }
+  return haar_from_normals(n);
+}
+
 const uint32_t DOMAIN_HOT = 0x80000000u, DOMAIN_GAUGE = 0x90000000u;
 
 // Reference-schedule chain state (one rank): lattice + mt19937_64.
@@ -563,6 +570,348 @@ struct RefChain {
     return l;
   }
 };
+
+// ---- event-chain Monte Carlo (src/ecmc/ecmc_mpi_cb.cpp, src/su3/utils.cpp) ----------------
+// Library form of mpi::ecmccb::sample_persistant (ecmc_mpi_cb.cpp:496-637): the lattice is
+// cut into blocks of edge l_core (one per MPI rank in the reference) and every block runs
+// its own persistent chain.  The chains are independent: the links a chain reads outside its
+// own active links are frozen in their owners' blocks (GeometryCB.cpp:33-56).  Randomness:
+// chain c's k-th uniform comes from Philox4x32-10 with counter (k_lo, k_hi, c, ECMC_CHAIN) and
+// key = seed; the set of SU(3) elements near the identity (ecmc_set) is drawn once per sample
+// call from counters (j, call_lo, call_hi, ECMC_SET) and shared by all chains.
+const uint32_t ECMC_CHAIN = 0xECEC0001u, ECMC_SET = 0xECEC0002u;
+const int ECMC_SET_SIZE = 10001;  // sample_persistant's set (ecmc_mpi_cb.cpp:560)
+const uint64_t ECMC_MAX_EVENTS = 1ull << 26;
+
+// Same layout as qcb_ecmc_chain in the library's C header.
+struct EcmcChain {
+  double R[18];
+  double theta_refresh_site, theta_refresh_R;
+  double travelled_site, travelled_R;
+  uint64_t draws, events, lifts, revs;
+  int32_t site[4];
+  int32_t mu, epsilon, initialized, status;
+  int32_t pad[4];
+};
+static_assert(sizeof(EcmcChain) == 256, "chain record is 256 bytes");
+
+struct EcmcParams {
+  double beta, theta_sample, theta_refresh_site, theta_refresh_R, epsilon_set;
+  int poisson, l_core;
+};
+
+// Uniform in (0, 1) from two 32-bit words: (top 53 bits of hi:lo + 1/2) 2^-53.
+static double u53(uint32_t lo, uint32_t hi) {
+  const uint64_t x = ((((uint64_t)hi) << 32) | lo) >> 11;
+  return ((double)x + 0.5) * 1.1102230246251565e-16;
+}
+
+struct EcmcStream {
+  uint32_t chain, k0, k1;
+  uint64_t* draws;
+  double uni() {
+    const uint64_t n = (*draws)++;
+    P4 r = philox({{(uint32_t)n, (uint32_t)(n >> 32), chain, ECMC_CHAIN}}, k0, k1);
+    return u53(r.v[0], r.v[1]);
+  }
+  // random_su3 (src/su3/utils.cpp:13-30) redrawn: Haar SU(3) from 12 Box-Muller normals.
+  M3 haar() {
+    double n[12];
+    for (int k = 0; k < 6; ++k) {
+      const double u1 = uni(), u2 = uni();
+      const double rad = sqrt(-2.0 * log(u1));
+      n[2 * k] = rad * cos(2 * M_PI * u2);
+      n[2 * k + 1] = rad * sin(2 * M_PI * u2);
+    }
+    return haar_from_normals(n);
+  }
+};
+
+// random_SU3_epsilon (src/su3/utils.cpp:66-105): product of the SU(2) elements
+// (sqrt(1 - eps^2), eps r/|r|) embedded in subgroups (0,1), (0,2), (1,2), r from (-1/2, 1/2)^3.
+static M3 su3_near_identity(double eps, const double r[9]) {
+  static const int sub[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+  M3 M = ident();
+  for (int s = 0; s < 3; ++s) {
+    const double r1 = r[3 * s], r2 = r[3 * s + 1], r3 = r[3 * s + 2];
+    const double norm = sqrt(r1 * r1 + r2 * r2 + r3 * r3);
+    Q4 x = {{sqrt(1 - eps * eps), eps * r1 / norm, eps * r2 / norm, eps * r3 / norm}};
+    M = mul(M, su2_quaternion_to_su3(x, sub[s][0], sub[s][1]));
+  }
+  return M;
+}
+
+// ecmc_set (src/su3/utils.cpp:119-127): set[0] = 1, set[2p+1] = random_SU3_epsilon,
+// set[2p+2] = its adjoint.
+static void ecmc_set(double eps, uint64_t seed, uint64_t call, std::vector<M3>& set) {
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  set.assign(ECMC_SET_SIZE, ident());
+  for (int p = 0; p < (ECMC_SET_SIZE - 1) / 2; ++p) {
+    double r[9];
+    for (int d = 0; d < 9; ++d) {
+      P4 w = philox({{(uint32_t)(p * 9 + d), (uint32_t)call, (uint32_t)(call >> 32), ECMC_SET}}, k0, k1);
+      r[d] = u53(w.v[0], w.v[1]) - 0.5;
+    }
+    set[2 * p + 1] = su3_near_identity(eps, r);
+    set[2 * p + 2] = adj(set[2 * p + 1]);
+  }
+}
+
+// solve_reject_fast (ecmc_mpi_cb.h:59-94): along U(theta) = R diag(e^{i eps theta},
+// e^{-i eps theta}, 1) R^dagger U one staple's action is A cos(theta) + eps B sin(theta) + const;
+// returns the angle at which the integral of the positive part of its derivative reaches gamma.
+static double solve_reject(double A, double B, double gamma, int eps) {
+  if (eps == -1) B = -B;
+  const double R = hypot(A, B), invR = 1.0 / R, period = 2.0 * R;
+  const double disc = floor(gamma / period);
+  gamma -= disc * period;
+  double phi = atan2(-A, B);
+  if (phi < 0.0) phi += 2.0 * M_PI;
+  const double p1 = R - A;
+  double alpha;
+  if (phi < M_PI * 0.5 || phi > M_PI * 1.5)
+    alpha = (gamma > p1) ? (gamma - p1) * invR - 1.0 : (gamma + A) * invR;
+  else
+    alpha = gamma * invR - 1.0;
+  alpha = alpha > 1.0 ? 1.0 : (alpha < -1.0 ? -1.0 : alpha);
+  double theta = phi + asin(alpha);
+  if (theta < 0.0) theta += 2.0 * M_PI;
+  if (theta >= 2.0 * M_PI) theta -= 2.0 * M_PI;
+  return theta + 2.0 * M_PI * disc;
+}
+
+// compute_reject_angles_fast (ecmc_mpi_cb.cpp:197-246), one staple S with T = R^dagger U:
+// P = T S R, A = -(beta/3) Re(P00 + P11), B = -(beta/3) Im(P11 - P00).
+static double reject_angle(const M3& T, const M3& S, const M3& R, double beta, double gamma, int eps) {
+  C m0[3], m1[3];
+  for (int c = 0; c < 3; ++c) {
+    m0[c] = T(0, 0) * S(0, c) + T(0, 1) * S(1, c) + T(0, 2) * S(2, c);
+    m1[c] = T(1, 0) * S(0, c) + T(1, 1) * S(1, c) + T(1, 2) * S(2, c);
+  }
+  const C P00 = m0[0] * R(0, 0) + m0[1] * R(1, 0) + m0[2] * R(2, 0);
+  const C P11 = m1[0] * R(0, 1) + m1[1] * R(1, 1) + m1[2] * R(2, 1);
+  const double br = -(beta / 3.0);
+  return solve_reject((P00.real() + P11.real()) * br, (P11.imag() - P00.imag()) * br, gamma, eps);
+}
+
+// compute_ds (ecmc_mpi_cb.cpp:263-274): Im[(R^dagger P R)_00 - (R^dagger P R)_11].
+static double compute_ds(const M3& P, const M3& R) {
+  M3 M = mul(P, R);
+  C res = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    res += std::conj(R(k, 0)) * M(k, 0);
+    res -= std::conj(R(k, 1)) * M(k, 1);
+  }
+  return res.imag();
+}
+
+static int dsign(double x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
+
+// One chain's block: block coordinates b, the lattice, and the cumulative shift of the
+// field's frame.  Local coordinates lc (each in [-1, l]; -1 and l are the neighbours' faces,
+// the reference's halo) map to the stored site b_d l + lc_d - cum_d (mod L_d).
+struct EcmcBlock {
+  Lat* f;
+  int l, b[4], cum[4];
+  size_t site(const int lc[4]) const {
+    int c[4];
+    for (int d = 0; d < 4; ++d) c[d] = ((b[d] * l + lc[d] - cum[d]) % f->L[d] + f->L[d]) % f->L[d];
+    return f->idx(c[0], c[1], c[2], c[3]);
+  }
+  M3 get(const int lc[4], int mu) const { return f->get(site(lc), mu); }
+  // GeometryCB::is_frozen in block-local terms: the halo (outside [0, l)) and the links
+  // leaving local coordinate 0 in a direction d != mu.
+  bool frozen(const int lc[4], int mu) const {
+    for (int d = 0; d < 4; ++d)
+      if (lc[d] < 0 || lc[d] >= l || (d != mu && lc[d] == 0)) return true;
+    return false;
+  }
+};
+
+static void shifted(const int a[4], int d1, int s1, int d2, int s2, int out[4]) {
+  for (int d = 0; d < 4; ++d) out[d] = a[d];
+  if (d1 >= 0) out[d1] += s1;
+  if (d2 >= 0) out[d2] += s2;
+}
+
+// sample_persistant (ecmc_mpi_cb.cpp:496-637) for one chain: events until the chain has
+// travelled theta_sample; the state persists across calls.  The set of near-identity
+// elements is the call's shared set (the reference regenerates its per-rank set at every
+// call and every 10000 lifts).
+static void ecmc_chain(const EcmcBlock& blk, const EcmcParams& p, const std::vector<M3>& set, uint32_t chain,
+                       uint64_t seed, EcmcChain& st) {
+  Lat& f = *blk.f;
+  const int l = p.l_core;
+  EcmcStream g{chain, (uint32_t)seed, (uint32_t)(seed >> 32), &st.draws};
+  // random_site (ecmc_mpi_cb.cpp:359-367): local coordinates 1 .. l-2 (padded 2 .. L-1)
+  auto rand_site = [&](int lc[4]) {
+    for (int d = 0; d < 4; ++d) lc[d] = 1 + (int)(g.uni() * (double)(l - 2));
+  };
+  M3 R;
+  if (!st.initialized) {
+    rand_site(st.site);
+    st.mu = (int)(g.uni() * 4.0);
+    st.epsilon = g.uni() < 0.5 ? -1 : 1;
+    R = g.haar();
+    st.theta_refresh_site = p.poisson ? -log(g.uni()) * p.theta_refresh_site : p.theta_refresh_site;
+    st.theta_refresh_R = p.poisson ? -log(g.uni()) * p.theta_refresh_R : p.theta_refresh_R;
+    st.travelled_site = st.travelled_R = 0.0;
+    st.events = st.lifts = 0;
+    st.initialized = 1;
+  } else {
+    memcpy(R.a, st.R, sizeof R.a);
+  }
+  const double theta_sample = p.poisson ? -log(g.uni()) * p.theta_sample : p.theta_sample;
+  double trav_sample = 0.0;
+  int lc[4] = {st.site[0], st.site[1], st.site[2], st.site[3]};
+  int mu = st.mu, eps = st.epsilon;
+  for (uint64_t ev = 0;; ++ev) {
+    if (ev >= ECMC_MAX_EVENTS) {
+      st.status |= 2;
+      break;
+    }
+    const size_t x = blk.site(lc);
+    const M3 U = f.get(x, mu);
+    const M3 T = mul(adj(R), U);
+    // compute_list_staples (ecmc_mpi_cb.cpp:12-36): for each nu != mu, forward then backward
+    double best = 0.0;
+    int j = 0, k = 0;
+    for (int nu = 0; nu < 4; ++nu) {
+      if (nu == mu) continue;
+      int a[4], c[4], d[4], e[4];
+      shifted(lc, mu, 1, -1, 0, a);   // x+mu
+      shifted(lc, nu, 1, -1, 0, c);   // x+nu
+      shifted(lc, mu, 1, nu, -1, d);  // x+mu-nu
+      shifted(lc, nu, -1, -1, 0, e);  // x-nu
+      M3 S = mul(blk.get(a, nu), adj(mul(f.get(x, nu), blk.get(c, mu))));
+      double rej = reject_angle(T, S, R, p.beta, -log(g.uni()), eps);
+      if (k == 0 || rej < best) best = rej, j = k;
+      ++k;
+      S = mul(adj(mul(blk.get(e, mu), blk.get(d, nu))), blk.get(e, nu));
+      rej = reject_angle(T, S, R, p.beta, -log(g.uni()), eps);
+      if (rej < best) best = rej, j = k;
+      ++k;
+    }
+    const double d_sample = theta_sample - trav_sample;
+    const double d_site = st.theta_refresh_site - st.travelled_site;
+    const double d_R = st.theta_refresh_R - st.travelled_R;
+    const double step = std::min({best, d_sample, d_site, d_R});
+    if (!std::isfinite(step)) {
+      st.status |= 1;
+      break;
+    }
+    // update (ecmc_mpi_cb.cpp:340-356): U <- R diag(e^{i xi}, e^{-i xi}, 1) R^dagger U, xi = eps theta
+    auto update = [&](double theta) {
+      const double xi = eps * theta, cs = cos(xi), sn = sin(xi);
+      M3 T2 = T;
+      for (int cc = 0; cc < 3; ++cc) {
+        T2(0, cc) *= C(cs, sn);
+        T2(1, cc) *= C(cs, -sn);
+      }
+      f.set(x, mu, mul(R, T2));
+      st.events++;
+    };
+    if (step == d_sample) {
+      update(d_sample);
+      st.travelled_site += d_sample;
+      st.travelled_R += d_sample;
+      break;
+    } else if (step == d_site) {
+      update(d_site);
+      trav_sample += d_site;
+      st.travelled_R += d_site;
+      st.travelled_site = 0.0;
+      if (p.poisson) st.theta_refresh_site = -log(g.uni()) * p.theta_refresh_site;
+      rand_site(lc);
+      mu = (int)(g.uni() * 4.0);
+      eps = g.uni() < 0.5 ? -1 : 1;
+    } else if (step == d_R) {
+      update(d_R);
+      trav_sample += d_R;
+      st.travelled_site += d_R;
+      st.travelled_R = 0.0;
+      if (p.poisson) st.theta_refresh_R = -log(g.uni()) * p.theta_refresh_R;
+      R = g.haar();
+    } else {
+      update(best);
+      trav_sample += best;
+      st.travelled_site += best;
+      st.travelled_R += best;
+      // lift_improved_fast (ecmc_mpi_cb.cpp:277-337) on plaquette j; its links
+      // (GeometryCB.cpp:58-90): 0 = (x, mu); forward 1 = (x+mu, nu), 2 = (x+nu, mu),
+      // 3 = (x, nu); backward 1 = (x+mu-nu, nu), 2 = (x-nu, mu), 3 = (x-nu, nu).
+      int nu = 0;
+      for (int q = 0, n = 0; q < 4; ++q)
+        if (q != mu) {
+          if (n == j / 2) nu = q;
+          ++n;
+        }
+      const bool fwd = (j % 2) == 0;
+      int lk[4][4], ld[4] = {mu, nu, mu, nu};
+      shifted(lc, -1, 0, -1, 0, lk[0]);
+      if (fwd) {
+        shifted(lc, mu, 1, -1, 0, lk[1]);
+        shifted(lc, nu, 1, -1, 0, lk[2]);
+        shifted(lc, -1, 0, -1, 0, lk[3]);
+      } else {
+        shifted(lc, mu, 1, nu, -1, lk[1]);
+        shifted(lc, nu, -1, -1, 0, lk[2]);
+        shifted(lc, nu, -1, -1, 0, lk[3]);
+      }
+      const M3 U0 = f.get(x, mu), U1 = blk.get(lk[1], nu), U2 = blk.get(lk[2], mu), U3 = blk.get(lk[3], nu);
+      M3 P[4];
+      if (fwd) {
+        const M3 U01 = mul(U0, U1), U32 = mul(U3, U2);
+        P[0] = mul(U01, adj(U32));
+        P[1] = mul(mul(U1, adj(U32)), U0);
+        P[2] = mul(mul(U2, adj(U01)), U3);
+        P[3] = adj(P[0]);
+      } else {
+        const M3 U21 = mul(U2, U1), Tb = mul(U0, adj(U21));
+        P[0] = mul(Tb, U3);
+        P[1] = mul(mul(mul(U1, adj(U0)), adj(U3)), U2);
+        P[3] = mul(U3, Tb);
+        P[2] = adj(P[3]);
+      }
+      double ab[4], sum = 0.0;
+      int sg[4];
+      for (int i = 0; i < 4; ++i) {
+        const double ds = blk.frozen(lk[i], ld[i]) ? 0.0 : compute_ds(P[i], R);
+        sg[i] = dsign(ds);
+        ab[i] = fabs(ds);
+        sum += ab[i];
+      }
+      double pr[4];
+      for (int i = 0; i < 4; ++i) pr[i] = ab[i] / sum;
+      // selectVariable (ecmc_mpi_cb.cpp:252-260)
+      const double r = g.uni();
+      const int idx = r < pr[0] ? 0 : (r < pr[0] + pr[1] ? 1 : (r < pr[0] + pr[1] + pr[2] ? 2 : 3));
+      const int iset = (int)(g.uni() * (double)ECMC_SET_SIZE);
+      const M3 Rn = mul(set[iset], R);
+      const double ds_old = sg[idx] * ab[idx];
+      const double ds_new = compute_ds(P[idx], Rn);
+      int new_eps = -sg[idx];
+      if (fabs(ds_old) < fabs(ds_new)) {
+        R = Rn;
+        new_eps = -dsign(ds_new);
+      } else if (g.uni() < fabs(ds_new) / fabs(ds_old)) {
+        R = Rn;
+        new_eps = -dsign(ds_new);
+      }
+      bool same = true;
+      for (int d = 0; d < 4; ++d) same = same && (lk[idx][d] == lc[d]);
+      st.revs += same ? 1 : 0;
+      st.lifts++;
+      for (int d = 0; d < 4; ++d) lc[d] = lk[idx][d];
+      mu = ld[idx];
+      eps = new_eps;
+    }
+  }
+  for (int d = 0; d < 4; ++d) st.site[d] = lc[d];
+  st.mu = mu;
+  st.epsilon = eps;
+  memcpy(st.R, R.a, sizeof R.a);
+}
 
 }  // namespace orc
 
@@ -751,6 +1100,59 @@ int orc_ref_get_links(void* h, double* aos) {
 int orc_ref_set_links(void* h, const double* aos) {
   RefChain* c = static_cast<RefChain*>(h);
   memcpy(c->links.data(), aos, c->links.size() * sizeof(C));
+  return 0;
+}
+
+// ---- event-chain Monte Carlo --------------------------------------------------------------
+int orc_ecmc_solve_reject(double A, double B, double gamma, int eps, double* out) {
+  *out = solve_reject(A, B, gamma, eps);
+  return 0;
+}
+
+int orc_ecmc_compute_ds(const double* p18, const double* r18, double* out) {
+  M3 P, R;
+  memcpy(P.a, p18, sizeof P.a);
+  memcpy(R.a, r18, sizeof R.a);
+  *out = compute_ds(P, R);
+  return 0;
+}
+
+// The call's set of ECMC_SET_SIZE matrices (18 doubles each).
+int orc_ecmc_set(double eps, uint64_t seed, uint64_t call, double* out) {
+  std::vector<M3> set;
+  ecmc_set(eps, seed, call, set);
+  for (int i = 0; i < ECMC_SET_SIZE; ++i) memcpy(out + 18 * i, set[i].a, sizeof set[i].a);
+  return 0;
+}
+
+// One sample call of every chain.  dp = {beta, theta_sample, theta_refresh_site,
+// theta_refresh_R, epsilon_set}, ip = {poisson, l_core}; cum = cumulative shift of the field's
+// frame; chains = prod(dims / l_core) records, chain id ((bx nby + by) nbz + bz) nbt + bt.
+int orc_ecmc_sample(double* aos, const int dims[4], const double dp[5], const int ip[2], uint64_t seed, uint64_t call,
+                    const int cum[4], void* chains) {
+  Lat f = make(aos, dims);
+  EcmcParams p{dp[0], dp[1], dp[2], dp[3], dp[4], ip[0], ip[1]};
+  const int l = p.l_core;
+  int nb[4];
+  for (int d = 0; d < 4; ++d) {
+    if (l < 3 || dims[d] % l) return 1;
+    nb[d] = dims[d] / l;
+  }
+  std::vector<M3> set;
+  ecmc_set(p.epsilon_set, seed, call, set);
+  EcmcChain* st = static_cast<EcmcChain*>(chains);
+  EcmcBlock blk;
+  blk.f = &f;
+  blk.l = l;
+  for (int d = 0; d < 4; ++d) blk.cum[d] = ((cum[d] % dims[d]) + dims[d]) % dims[d];
+  uint32_t id = 0;
+  for (int bx = 0; bx < nb[0]; ++bx)
+    for (int by = 0; by < nb[1]; ++by)
+      for (int bz = 0; bz < nb[2]; ++bz)
+        for (int bt = 0; bt < nb[3]; ++bt, ++id) {
+          blk.b[0] = bx, blk.b[1] = by, blk.b[2] = bz, blk.b[3] = bt;
+          ecmc_chain(blk, p, set, id, seed, st[id]);
+        }
   return 0;
 }
 

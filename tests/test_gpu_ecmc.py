@@ -1,0 +1,178 @@
+"""Event-chain Monte Carlo on the GPU (qcb_ecmc_*) against the oracle's restatement of
+mpi::ecmccb::sample_persistant (src/ecmc/ecmc_mpi_cb.cpp:496-637).
+
+Both draw every random number from the same Philox counters, so the GPU chains take the
+oracle's events one for one: counters, positions and draw counts agree exactly, links and
+chain matrices to rounding.  Plus: frozen links stay bit-identical, FP32 storage, resume
+from saved records, argument checks, and the equilibrium plaquette against the heatbath.
+"""
+import numpy as np
+import pytest
+
+import oracle as orc
+import qcb
+from qcb.ecmc import CHAIN_DTYPE
+
+pytestmark = pytest.mark.gpu
+
+BASE = dict(beta=6.0, theta_sample=20.0, theta_refresh_site=10.0, theta_refresh_R=3.0, epsilon_set=0.15,
+            poisson=0, l_core=4)
+EXACT = ["draws", "events", "lifts", "revs", "site", "mu", "epsilon", "initialized", "status"]
+
+
+def _compare(rec, ref, tol=1e-9):
+    for k in EXACT:
+        assert np.array_equal(rec[k], ref[k]), k
+    for k in ("R", "theta_refresh_site", "theta_refresh_R", "travelled_site", "travelled_R"):
+        assert np.abs(rec[k] - ref[k]).max() < tol, k
+
+
+@pytest.mark.parametrize("dims,l,poisson,beta", [((8, 8, 8, 8), 4, 0, 6.0), ((6, 6, 12, 6), 3, 1, 5.7),
+                                                ((8, 8, 8, 16), 4, 0, 2.0)])
+def test_matches_oracle_event_for_event(ctx, dims, l, poisson, beta):
+    p = dict(BASE, l_core=l, poisson=poisson, beta=beta)
+    u = orc.hot_philox(dims, 21)
+    f = qcb.GaugeField(ctx, dims)
+    f.set_links(u)
+    ch = qcb.EventChains(f, p, 77)
+    ref_u, ref_c = u, orc.ecmc_chains(dims, l)
+    rng = np.random.default_rng(4)
+    cum = np.zeros(4, int)
+    for call in range(4):
+        cum = (cum + rng.integers(0, l, 4)) % np.array(dims)
+        ch.sample(cum)
+        ref_u, ref_c = orc.ecmc_sample(ref_u, dims, p, 77, call, cum, ref_c)
+        rec, calls = ch.chains()
+        assert calls == call + 1
+        _compare(rec, ref_c)
+        assert np.abs(f.get_links() - ref_u).max() < 1e-9
+    ev, lifts, revs = ch.counters()
+    assert (ev, lifts, revs) == (int(ref_c["events"].sum()), int(ref_c["lifts"].sum()), int(ref_c["revs"].sum()))
+    ch.close()
+    f.close()
+
+
+def test_frozen_links_bit_identical(ctx):
+    dims, l, cum = (8, 8, 8, 8), 4, (3, 1, 0, 2)
+    u = orc.hot_philox(dims, 2)
+    f = qcb.GaugeField(ctx, dims)
+    f.set_links(u)
+    ch = qcb.EventChains(f, BASE, 5)
+    ch.sample(cum)
+    got = f.get_links()
+    lx, ly, lz, lt = dims
+    t, z, y, x = np.meshgrid(np.arange(lt), np.arange(lz), np.arange(ly), np.arange(lx), indexing="ij")
+    c = [x, y, z, t]
+    for mu in range(4):
+        frozen = np.zeros((lt, lz, ly, lx), bool)
+        for d in range(4):
+            if d != mu:
+                frozen |= (c[d] + cum[d]) % l == 0
+        assert np.array_equal(got[frozen, mu], u[frozen, mu])
+        assert not np.array_equal(got[~frozen, mu], u[~frozen, mu])
+    ch.close()
+    f.close()
+
+
+def test_fp32_storage_tracks_fp64(ctx):
+    dims = (8, 8, 8, 8)
+    u = orc.hot_philox(dims, 8)
+    f = qcb.GaugeField(ctx, dims, "fp32", 12)
+    f.set_links(u)
+    ch = qcb.EventChains(f, BASE, 9)
+    ch.sample((1, 1, 1, 1))
+    # the chains see the FP32-rounded start, so compare with the oracle from the same start
+    start = qcb.GaugeField(ctx, dims, "fp32", 12)
+    start.set_links(u)
+    u32 = start.get_links()
+    ref_u, ref_c = orc.ecmc_sample(u32, dims, BASE, 9, 0, (1, 1, 1, 1), orc.ecmc_chains(dims, 4))
+    rec, _ = ch.chains()
+    assert np.array_equal(rec["events"], ref_c["events"])
+    assert np.abs(f.get_links() - ref_u).max() < 1e-5
+    for o in (ch, f, start):
+        o.close()
+
+
+def test_resume_from_saved_records(ctx):
+    dims = (8, 8, 8, 8)
+    u = orc.hot_philox(dims, 6)
+    f = qcb.GaugeField(ctx, dims)
+    f.set_links(u)
+    a = qcb.EventChains(f, BASE, 31)
+    a.sample((0, 1, 2, 3))
+    rec, calls = a.chains()
+    mid = f.get_links()
+    a.sample((2, 2, 2, 2))
+    want = f.get_links()
+    f.set_links(mid)
+    b = qcb.EventChains(f, BASE, 31)
+    b.set_chains(rec, calls)
+    b.sample((2, 2, 2, 2))
+    assert np.array_equal(f.get_links(), want)
+    assert np.array_equal(b.chains()[0], a.chains()[0])
+    for o in (a, b, f):
+        o.close()
+
+
+def test_counters_reset(ctx):
+    dims = (8, 8, 8, 8)
+    f = qcb.GaugeField(ctx, dims)
+    f.hot_start(3)
+    ch = qcb.EventChains(f, BASE, 1)
+    ch.sample()
+    ev, lifts, revs = ch.counters(reset=True)
+    assert ev >= lifts > revs > 0
+    assert ch.counters() == (0, 0, 0)
+    ch.sample((1, 0, 0, 0))
+    assert ch.counters()[0] > 0
+    ch.close()
+    f.close()
+
+
+def test_argument_checks(ctx):
+    f = qcb.GaugeField(ctx, (8, 8, 8, 8))
+    for bad in (dict(BASE, l_core=2), dict(BASE, l_core=3), dict(BASE, beta=0.0), dict(BASE, theta_sample=-1.0),
+                dict(BASE, epsilon_set=1.5)):
+        with pytest.raises(qcb.QcbError) as e:
+            qcb.EventChains(f, bad, 1)
+        assert e.value.code == 1
+    ch = qcb.EventChains(f, BASE, 1)
+    rec = np.zeros(ch.n_chains, CHAIN_DTYPE)
+    rec["initialized"] = 1
+    rec["mu"] = 4
+    with pytest.raises(qcb.QcbError) as e:
+        ch.set_chains(rec, 0)
+    assert e.value.code == 1
+    ch.close()
+    f.close()
+
+
+def test_equilibrium_matches_heatbath(ctx):
+    """From a heatbath-equilibrated 8^4 field at beta = 6.0, the ECMC keeps the heatbath's
+    mean plaquette (within the combined statistical error)."""
+    dims, beta = (8, 8, 8, 8), 6.0
+    f = qcb.GaugeField(ctx, dims)
+    f.cold_start()
+    hp = []
+    for s in range(1200):
+        qcb._lib.check(qcb._lib.lib().qcb_heatbath(f.h, beta, 1, 1, 13, s))
+        if s >= 200:
+            hp.append(qcb.observables.mean_plaquette_global(f))
+    ch = qcb.EventChains(f, dict(BASE, theta_sample=100.0, theta_refresh_site=50.0, theta_refresh_R=15.0), 19)
+    rng = np.random.default_rng(5)
+    cum = np.zeros(4, int)
+    ep = []
+    for call in range(3000):
+        cum = (cum + rng.integers(0, 4, 4)) % 8
+        ch.sample(cum)
+        if call >= 500:
+            ep.append(qcb.observables.mean_plaquette_global(f))
+
+    def err(x, nb=20):
+        x = np.asarray(x)
+        n = len(x) // nb
+        return x[:n * nb].reshape(nb, n).mean(1).std() / np.sqrt(nb)
+
+    assert abs(np.mean(ep) - np.mean(hp)) < 4 * np.hypot(err(ep), err(hp)), (np.mean(ep), np.mean(hp))
+    ch.close()
+    f.close()

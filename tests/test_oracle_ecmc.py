@@ -1,0 +1,164 @@
+"""CPU checks of the oracle's event-chain Monte Carlo (restatement of
+src/ecmc/ecmc_mpi_cb.cpp): the reject-angle equation, dS, the near-identity set, the block
+decomposition (frozen links never move, chains stay in their blocks) and, statistically,
+the equilibrium it samples against the heatbath."""
+import numpy as np
+import pytest
+
+import oracle as orc
+
+LAMBDA3 = np.diag([1.0, -1.0, 0.0])
+
+
+def _pos_integral(A, B, eps, theta, n=400001):
+    """int_0^theta max(0, dS/dt) dt for S(t) = A cos t + eps B sin t (dense trapezoid)."""
+    t = np.linspace(0.0, theta, n)
+    d = np.maximum(0.0, -A * np.sin(t) + eps * B * np.cos(t))
+    return float(np.sum((d[1:] + d[:-1]) * 0.5 * np.diff(t)))
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_solve_reject_integral(seed):
+    """The reject angle is where the accumulated positive part of the staple's dS/dtheta
+    reaches gamma (the factorized Metropolis filter), for both senses of rotation."""
+    rng = np.random.default_rng(seed)
+    for _ in range(20):
+        A, B = rng.normal(0, 2.0, 2)
+        gamma = rng.exponential(1.0) * (1.0 + 3 * rng.random())
+        for eps in (-1, 1):
+            th = orc.ecmc_solve_reject(A, B, gamma, eps)
+            assert th >= 0.0
+            got = _pos_integral(A, B, eps, th)
+            assert abs(got - gamma) < 2e-4 * max(1.0, gamma), (A, B, gamma, eps, th, got)
+
+
+def test_solve_reject_periods():
+    """gamma beyond one period (2 R) adds whole turns of 2 pi."""
+    A, B = 0.3, -0.7
+    R = np.hypot(A, B)
+    t1 = orc.ecmc_solve_reject(A, B, 0.25 * R, 1)
+    t2 = orc.ecmc_solve_reject(A, B, 0.25 * R + 3 * 2 * R, 1)
+    assert abs(t2 - t1 - 3 * 2 * np.pi) < 1e-9
+
+
+def _su3(rng):
+    z = rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3))
+    q, r = np.linalg.qr(z)
+    q = q * (np.diag(r) / np.abs(np.diag(r)))
+    return q / np.linalg.det(q) ** (1 / 3)
+
+
+def test_compute_ds_definition():
+    rng = np.random.default_rng(3)
+    for _ in range(10):
+        P = rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3))
+        R = _su3(rng)
+        want = np.trace(LAMBDA3 @ R.conj().T @ P @ R).imag
+        assert abs(orc.ecmc_compute_ds(P, R) - want) < 1e-12
+
+
+def test_set_structure():
+    s = orc.ecmc_set(0.15, 7, 3)
+    assert s.shape == (orc.ECMC_SET_SIZE, 3, 3)
+    assert np.allclose(s[0], np.eye(3))
+    assert np.allclose(s[2::2], np.conj(np.transpose(s[1::2], (0, 2, 1))))
+    uu = np.einsum("nij,nkj->nik", s, s.conj())
+    assert np.abs(uu - np.eye(3)).max() < 1e-13
+    assert np.abs(np.linalg.det(s) - 1).max() < 1e-13
+    dist = np.linalg.norm((s[1:] - np.eye(3)).reshape(len(s) - 1, -1), axis=1)
+    assert 0.1 < dist.mean() < 0.5  # three SU(2) rotations of size 0.15 each
+    assert not np.allclose(orc.ecmc_set(0.15, 7, 4)[1], s[1])  # a new set per call
+
+
+PARAMS = dict(beta=6.0, theta_sample=20.0, theta_refresh_site=10.0, theta_refresh_R=3.0, epsilon_set=0.15,
+              poisson=0, l_core=4)
+
+
+def _frozen_mask(dims, l, cum):
+    """(Lt, Lz, Ly, Lx, 4) mask of the links frozen by the l-block faces after shift cum."""
+    lx, ly, lz, lt = dims
+    t, z, y, x = np.meshgrid(np.arange(lt), np.arange(lz), np.arange(ly), np.arange(lx), indexing="ij")
+    c = [x, y, z, t]
+    m = np.zeros((lt, lz, ly, lx, 4), bool)
+    for mu in range(4):
+        for d in range(4):
+            if d != mu:
+                m[..., mu] |= (c[d] + cum[d]) % l == 0
+    return m
+
+
+@pytest.mark.parametrize("dims,l,poisson", [((8, 8, 8, 8), 4, 0), ((6, 9, 6, 3), 3, 1)])
+def test_blocks_frozen_links_and_confinement(dims, l, poisson):
+    p = dict(PARAMS, l_core=l, poisson=poisson)
+    u = orc.hot_philox(dims, 5)
+    ch = orc.ecmc_chains(dims, l)
+    cum = np.zeros(4, int)
+    rng = np.random.default_rng(1)
+    for call in range(4):
+        cum = (cum + rng.integers(0, l, 4)) % np.array(dims)
+        before = u.copy()
+        u, ch = orc.ecmc_sample(u, dims, p, 11, call, cum, ch)
+        frozen = _frozen_mask(dims, l, cum)
+        assert np.array_equal(u[frozen], before[frozen])
+        assert not np.array_equal(u[~frozen], before[~frozen])
+        assert (ch["initialized"] == 1).all() and (ch["status"] == 0).all()
+        assert ((ch["site"] >= 0) & (ch["site"] < l)).all()
+        assert ((ch["mu"] >= 0) & (ch["mu"] < 4)).all() and set(np.unique(ch["epsilon"])) <= {-1, 1}
+        assert (ch["events"] >= ch["lifts"]).all() and (ch["lifts"] > 0).all()
+    U = u.reshape(-1, 3, 3)
+    assert np.abs(np.einsum("nij,nkj->nik", U, U.conj()) - np.eye(3)).max() < 1e-12
+    assert np.abs(np.linalg.det(U) - 1).max() < 1e-12
+
+
+def test_sample_is_deterministic():
+    """A sample call is a pure function of (links, chain records, seed, call, shift)."""
+    dims, l = (8, 8, 8, 8), 4
+    u = orc.hot_philox(dims, 9)
+    ch = orc.ecmc_chains(dims, l)
+    a, ca = orc.ecmc_sample(u, dims, PARAMS, 3, 0, (1, 2, 3, 0), ch)
+    b, cb = orc.ecmc_sample(u, dims, PARAMS, 3, 0, (1, 2, 3, 0), ch)
+    assert np.array_equal(a, b) and np.array_equal(ca, cb)
+    c, _ = orc.ecmc_sample(u, dims, PARAMS, 4, 0, (1, 2, 3, 0), ch)
+    assert not np.array_equal(a, c)
+
+
+def test_resume_is_exact():
+    """Two calls = one call, save the chain records, second call from them."""
+    dims = (8, 8, 8, 8)
+    u = orc.hot_philox(dims, 4)
+    ch = orc.ecmc_chains(dims, 4)
+    a1, c1 = orc.ecmc_sample(u, dims, PARAMS, 5, 0, (0, 1, 0, 2), ch)
+    a2, c2 = orc.ecmc_sample(a1, dims, PARAMS, 5, 1, (3, 1, 2, 2), c1)
+    saved = c1.copy()
+    b2, d2 = orc.ecmc_sample(a1.copy(), dims, PARAMS, 5, 1, (3, 1, 2, 2), saved)
+    assert np.array_equal(a2, b2) and np.array_equal(c2, d2)
+
+
+def test_equilibrium_matches_heatbath_strong_coupling():
+    """At beta = 2 (fast decorrelation) the ECMC plaquette agrees with the heatbath's on the
+    same 6^4 lattice within the combined statistical error."""
+    dims, beta = (6, 6, 6, 6), 2.0
+    uh = orc.cold(dims)
+    hp = []
+    for s in range(160):
+        uh, _ = orc.heatbath_cb(uh, dims, beta, 1, 1, 17, s)
+        if s >= 40:
+            hp.append(orc.plaquette(uh, dims))
+    p = dict(PARAMS, beta=beta, theta_sample=15.0, l_core=3)
+    u, ch = uh.copy(), orc.ecmc_chains(dims, 3)
+    rng = np.random.default_rng(8)
+    cum = np.zeros(4, int)
+    ep = []
+    for call in range(220):
+        cum = (cum + rng.integers(0, 3, 4)) % 6
+        u, ch = orc.ecmc_sample(u, dims, p, 23, call, cum, ch)
+        if call >= 20:
+            ep.append(orc.plaquette(u, dims))
+
+    def err(x, nb=10):
+        x = np.asarray(x)
+        n = len(x) // nb
+        return x[:n * nb].reshape(nb, n).mean(1).std() / np.sqrt(nb)
+
+    diff = abs(np.mean(ep) - np.mean(hp))
+    assert diff < 4 * np.hypot(err(ep), err(hp)) + 1e-4, (np.mean(ep), np.mean(hp), err(ep), err(hp))
