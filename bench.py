@@ -321,6 +321,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         rate = 0.8 * result["serving"]["throughput_jobs_per_s"]
         result["serving_80pct_load"] = serving_section(ctx, n_requests=40, rate=rate)
         result["plain"] = plain_section()
+        result["ecmc"] = ecmc_section(ctx, cpu=not args.no_cpu_baseline)
     return result
 
 
@@ -412,6 +413,114 @@ def batch_section(ctx, lib, stream):
                              "launches": 64 * 800},
             "autotune_s": tune_s, "tiles": {"hb": sorted(set(hb_tiles)), "flow": sorted(set(flow_tiles))},
             "mean_plaquette": float(np.mean(plaq)), "mean_E_t2": float(np.mean(rec[:, -1, 2]))}
+
+
+ECMC_L, ECMC_LCORE, ECMC_THETA = 64, 4, 100.0
+# FP64 operations of one ECMC event (a lift; refresh events are rarer and cheaper), counted
+# from the kernel's source: six staples (one SU(3) product, two projected columns and two
+# projected rows: 69 complex multiply-adds each), the update (two SU(3) products), the lift
+# (seven SU(3) products for three plaquettes, the set element times R, dS traces) and the
+# reject-angle solves (log, hypot, atan2, asin, a division: about 120 operations each).
+ECMC_FLOP_PER_EVENT = 8 * (6 * 69 + 2 * 27 + 8 * 27 + 6 * 9) + 6 * 120
+FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64 (non-tensor), NVIDIA's nominal figure; not measured here
+
+
+def _ecmc_cpu_worker(args):
+    """One host core: the oracle's chains on an 8^4 lattice of 4^4 blocks (16 chains, as the
+    reference's 16 ranks of inputs/ecold6.txt), calls of theta_sample = 100 until `budget` s."""
+    seed, budget = args
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import numpy as np
+
+    import oracle
+
+    dims = (8, 8, 8, 8)
+    p = dict(beta=BETA, theta_sample=ECMC_THETA, theta_refresh_site=50.0, theta_refresh_R=15.0, epsilon_set=0.15,
+             poisson=0, l_core=4)
+    u, _ = oracle.heatbath_cb(oracle.hot_philox(dims, seed), dims, BETA, 20, 1, seed, 0)
+    ch = oracle.ecmc_chains(dims, 4)
+    rng = np.random.default_rng(seed)
+    cum = np.zeros(4, int)
+    t = time.perf_counter()
+    call = 0
+    while time.perf_counter() - t < budget:
+        cum = (cum + rng.integers(0, 4, 4)) % 8
+        u, ch = oracle.ecmc_sample(u, dims, p, seed, call, cum, ch)
+        call += 1
+    return int(ch["events"].sum()), time.perf_counter() - t
+
+
+def ecmc_section(ctx, steps=5, warmup=3, cpu_budget_s=8.0, cpu=True):
+    """Event-chain Monte Carlo: a 64^4 FP64 lattice as 16^4 blocks of 4^4 (65536 chains, one
+    per block, as 65536 ranks of the reference would run), beta = 6.0, from a Haar hot start
+    (seed 7) plus 20 heatbath sweeps, with the reference's default budgets (theta_sample 100,
+    refresh site 50, refresh R 15, epsilon_set 0.15).  One step = one random translation and
+    one sample call of every chain (the links packed to the FP64 array-of-structures copy, the
+    set drawn, the chains run, the links unpacked); CUDA events on the library's stream."""
+    import numpy as np
+    import torch
+
+    import qcb
+
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    dims = (ECMC_L,) * 4
+    f = qcb.GaugeField(ctx, dims, "fp64", 18)
+    f.hot_start(SEED)
+    qcb._lib.check(qcb._lib.lib().qcb_heatbath(f.h, BETA, 20, 1, SEED, 0))
+    ch = qcb.EventChains(f, qcb.ecmc.params(beta=BETA, theta_sample=ECMC_THETA, l_core=ECMC_LCORE), SEED)
+    rng = np.random.default_rng(11)
+    cum = np.zeros(4, int)
+
+    def shift():
+        nonlocal cum
+        cum = (cum + rng.integers(0, ECMC_LCORE, 4)) % ECMC_L
+        ch.sample(cum)
+
+    for _ in range(warmup):
+        shift()
+    ch.counters(reset=True)
+    launches0 = ctx.launches()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        shift()
+    b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    launches = ctx.launches() - launches0
+    events, lifts, revs = ch.counters(reset=True)
+    rate = events / (ms / 1e3)
+    # end to end through the C ABI, the links resident: one shift + the plaquette to the host
+    t = time.perf_counter()
+    for _ in range(steps):
+        shift()
+        plaq = qcb.observables.mean_plaquette_global(f)
+    e2e_s = (time.perf_counter() - t) / steps
+    e_ev, _, _ = ch.counters(reset=True)
+    flop = ECMC_FLOP_PER_EVENT * rate / 1e12
+    out = {"metric": "ECMC events/s (one link update each)", "value": rate, "unit": "events/s",
+           "workload": f"{ECMC_L}^4 fp64, {ch.n_chains} chains of {ECMC_LCORE}^4 blocks, beta={BETA}, theta_sample="
+                       f"{ECMC_THETA:g}, refresh 50/15, epsilon_set 0.15",
+           "ms_per_step": ms / steps, "events_per_chain_per_step": events / steps / ch.n_chains,
+           "lambda": ECMC_THETA * ch.n_chains * steps / lifts, "same_site_lift_frac": revs / lifts,
+           "plaquette": plaq, "gpu_launches": launches,
+           "e2e": {"value": e_ev / (e2e_s * steps), "unit": "events/s", "s_per_step": e2e_s,
+                   "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8,
+                   "step": "random translation + qcb_ecmc_sample + qcb_plaquette to host, links resident"},
+           "roofline": {"bound": "fp64", "achieved": flop, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                        "frac": flop / FP64_NOMINAL_TFLOPS, "peak_kind": "nominal (no FP64 peak is measured)",
+                        "flop_per_event": ECMC_FLOP_PER_EVENT}}
+    ch.close()
+    f.close()
+    if cpu:
+        cores = min(64, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1))
+        with mp.get_context("spawn").Pool(cores) as pool:
+            res = pool.map(_ecmc_cpu_worker, [(500 + r, cpu_budget_s) for r in range(cores)])
+        out["cpu_baseline"] = {"value": sum(r[0] for r in res) / max(r[1] for r in res), "unit": "events/s",
+                               "cores": cores, "kind": "port",
+                               "sample": f"{cores} processes x the oracle's 16 chains on an 8^4 lattice of 4^4 "
+                                         f"blocks, theta_sample {ECMC_THETA:g} calls for {cpu_budget_s:g} s"}
+    return out
 
 
 def serving_section(ctx, n_requests=100, rate=20.0, quantum_sweeps=2, quantum_steps=4):
@@ -687,9 +796,9 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="run only warmup + steps of the workload (for ncu); print launch counts")
     ap.add_argument("--storage", choices=["fp32-12", "fp64-18"], default="fp32-12")
-    ap.add_argument("--workload", choices=["precision", "large", "batch"], default="precision",
+    ap.add_argument("--workload", choices=["precision", "large", "batch", "ecmc"], default="precision",
                     help="large: the 64^4 single-lattice workload; batch: the 64-lattice batching workload "
-                         "alone; each printed as its own JSON object")
+                         "alone; ecmc: the event-chain workload alone; each printed as its own JSON object")
     ap.add_argument("--out", default=None, help="also write the large-workload JSON to this path")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -732,6 +841,14 @@ def main():
             ctx = qcb.Context(0)
             stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
             print(json.dumps(batch_section(ctx, _lib.lib(), stream)))
+            ctx.close()
+        return 0
+    if args.workload == "ecmc":
+        if rank == 0:
+            import qcb
+
+            ctx = qcb.Context(0)
+            print(json.dumps(ecmc_section(ctx, steps=args.steps, warmup=args.warmup, cpu=not args.no_cpu_baseline)))
             ctx.close()
         return 0
     dist = replicas.init("nccl", timeout_s=300)

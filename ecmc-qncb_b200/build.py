@@ -1,9 +1,10 @@
-"""Build libqcb.so (sm_100a CUDA kernels + C ABI) and the gauge_hb_ncb driver in-tree.
+"""Build libqcb.so (sm_100a CUDA kernels + C ABI) and the gauge_hb_ncb / gauge_ecmc_ncb drivers
+in-tree.
 
     python ecmc-qncb_b200/build.py [--force] [-j N]
 
 Objects go to ecmc-qncb_b200/_build/, the library to ecmc-qncb_b200/lib/libqcb.so and the
-driver to ecmc-qncb_b200/bin/gauge_hb_ncb.  Every CUDA source is compiled for sm_100a only
+drivers to ecmc-qncb_b200/bin/.  Every CUDA source is compiled for sm_100a only
 (-gencode arch=compute_100a,code=sm_100a).  A target is rebuilt when a source or any
 header under csrc/ or include/ is newer than it.
 """
@@ -23,7 +24,8 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "lib" / "libqcb.so"
-DRIVER = PKG / "bin" / "gauge_hb_ncb"
+BIN = PKG / "bin"
+DRIVER = BIN / "gauge_hb_ncb"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # -prec-div=false / -prec-sqrt=false: FP32 division and square root by the hardware
@@ -32,7 +34,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # results are unchanged.
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
               "--expt-relaxed-constexpr", "-prec-div=false", "-prec-sqrt=false", "-I", str(INCLUDE)] + ARCH
-DRIVER_SOURCES = {"gauge_hb_ncb.cpp"}
+DRIVER_SOURCES = {"gauge_hb_ncb.cpp", "gauge_ecmc_ncb.cpp"}
 
 
 def nvcc() -> str:
@@ -91,10 +93,11 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
             list(ex.map(compile_one, todo))
     if force or todo or _stale(LIB, objs):
         _run([cc, "-shared", "-o", str(LIB)] + [str(o) for o in objs] + ARCH + ["-lpthread"])
-    drv_src = CSRC / "gauge_hb_ncb.cpp"
-    if drv_src.exists() and (force or _stale(DRIVER, [drv_src, LIB] + hdrs)):
-        _run([cc, "-x", "c++", str(drv_src), "-o", str(DRIVER), "-O2", "-std=c++17", "-I", str(INCLUDE),
-              "-L", str(LIB.parent), "-lqcb", "-Xlinker", "-rpath=$ORIGIN/../lib"])
+    for name in sorted(DRIVER_SOURCES):
+        drv_src, exe = CSRC / name, BIN / Path(name).stem
+        if drv_src.exists() and (force or _stale(exe, [drv_src, LIB] + hdrs)):
+            _run([cc, "-x", "c++", str(drv_src), "-o", str(exe), "-O2", "-std=c++17", "-I", str(INCLUDE),
+                  "-L", str(LIB.parent), "-lqcb", "-Xlinker", "-rpath=$ORIGIN/../lib"])
     return LIB
 
 

@@ -1002,4 +1002,40 @@ int qcb_params_load(const char* path, qcb_hb_params* p) {
   return QCB_OK;
 }
 
+int qcb_ecmc_run_params_default(qcb_ecmc_run_params* p) {
+  if (!p) return fail(QCB_ERR_INVALID, "null params");
+  memset(p, 0, sizeof *p);
+  // src/io/params.h:27-44 (RunParamsECB) and :9-17 (ECMCParams)
+  p->L_core = 6;
+  p->n_core_dims = 2;
+  p->cold_start = 1;
+  p->seed = 123;
+  p->N_shift = 2;
+  p->ecmc.beta = 6.0;
+  p->ecmc.theta_sample = 100.0;
+  p->ecmc.theta_refresh_site = 50.0;
+  p->ecmc.theta_refresh_R = 15.0;
+  p->ecmc.poisson = 0;
+  p->ecmc.epsilon_set = 0.15;
+  p->ecmc.l_core = 6;
+  p->N_therm = 100;
+  p->topo = 1;
+  p->N_shift_plaquette = 2;
+  p->N_shift_topo = 10;
+  p->N_steps_gf = 10;
+  p->N_rk_steps = 40;
+  strcpy(p->run_name, "c");
+  strcpy(p->run_dir, "data");
+  p->save_each_shifts = 2;
+  return QCB_OK;
+}
+
+int qcb_ecmc_run_params_load(const char* path, qcb_ecmc_run_params* p) {
+  if (!path || !p) return fail(QCB_ERR_INVALID, "null argument");
+  std::string err;
+  int r = ecmc_params_load(path, p, &err);
+  if (r != QCB_OK) return fail(r, err);
+  return QCB_OK;
+}
+
 }  // extern "C"

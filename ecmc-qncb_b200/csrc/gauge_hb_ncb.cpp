@@ -40,91 +40,20 @@
 #include <string>
 #include <vector>
 
+#include "driver_common.h"
 #include "qcb.h"
 
 namespace fs = std::filesystem;
+using drv::ensure_dir;
+using drv::fmt;
 
 namespace {
 
-[[noreturn]] void die(const std::string& what) {
-  std::cerr << "Error: " << what << ": " << qcb_last_error() << std::endl;
-  exit(1);
-}
-#define CHECK(call, what)                    \
-  do {                                       \
-    if ((call) != QCB_OK) die(what);         \
-  } while (0)
-
-std::string trim(const std::string& s) {
-  size_t a = s.find_first_not_of(" \t");
-  if (a == std::string::npos) return "";
-  size_t b = s.find_last_not_of(" \t");
-  return s.substr(a, b - a + 1);
-}
-
-// Extra keys that the reference does not know; parsed with the same line rules.
-std::map<std::string, std::string> extra_keys(const char* path) {
-  std::map<std::string, std::string> m;
-  std::ifstream f(path);
-  std::string line;
-  while (std::getline(f, line)) {
-    if (line.empty() || line[0] == '#') continue;
-    std::istringstream is(line);
-    std::string k, v;
-    if (std::getline(is, k, '=') && std::getline(is, v)) m[trim(k)] = trim(v);
-  }
-  return m;
-}
-
-std::string fmt(double v, int p) {
-  std::ostringstream ss;
-  ss << std::fixed << std::setprecision(p) << v;
-  return ss.str();
-}
-
-fs::path run_path(const qcb_hb_params& rp) { return fs::path(rp.run_dir) / rp.run_name; }
-
-void ensure_dir(const fs::path& d) {
-  std::error_code ec;
-  if (!fs::exists(d)) fs::create_directories(d, ec);
-  if (ec) std::cerr << "Couldn't create folder data : " << ec.message() << std::endl;
-}
-
-void save_plaquette(const std::vector<double>& data, const qcb_hb_params& rp) {
-  fs::path dir = run_path(rp);
-  ensure_dir(dir);
-  fs::path p = dir / (std::string(rp.run_name) + "_plaquette.txt");
-  std::ofstream f(p, std::ios::out | std::ios::app);
-  if (!f.is_open()) {
-    std::cout << "Could not open file " << p << "\n";
-    return;
-  }
-  f << std::fixed << std::setprecision(10);
-  for (double x : data) f << x << "\n";
-  std::cout << "Plaquette written in " << p << "\n";
-}
-
-void save_topo(const std::vector<double>& tQE, const qcb_hb_params& rp) {
-  fs::path dir = run_path(rp);
-  ensure_dir(dir);
-  fs::path p = dir / (std::string(rp.run_name) + "_topo.txt");
-  std::ofstream f(p, std::ios::out | std::ios::app);
-  if (!f.is_open()) {
-    std::cout << "Could not open file " << p << "\n";
-    return;
-  }
-  f << std::fixed << std::setprecision(10);
-  for (size_t i = 0; i + 2 < tQE.size(); i += 3)
-    f << tQE[i] << " " << tQE[i + 1] << " " << tQE[i + 2] << "\n";
-  std::cout << "Topology written in " << p << "\n";
-}
-
-void append_params_line(const qcb_hb_params& rp, const std::string& line) {
-  fs::path dir = run_path(rp);
-  ensure_dir(dir);
-  std::ofstream f(dir / (std::string(rp.run_name) + "_params.txt"), std::ios::out | std::ios::app);
-  if (f.is_open()) f << line;
-}
+drv::RunDir run_dir(const qcb_hb_params& rp) { return drv::RunDir{rp.run_dir, rp.run_name}; }
+fs::path run_path(const qcb_hb_params& rp) { return run_dir(rp).path(); }
+void save_plaquette(const std::vector<double>& data, const qcb_hb_params& rp) { drv::save_plaquette(data, run_dir(rp)); }
+void save_topo(const std::vector<double>& tQE, const qcb_hb_params& rp) { drv::save_topo(tQE, run_dir(rp)); }
+void append_params_line(const qcb_hb_params& rp, const std::string& line) { drv::append_params_line(run_dir(rp), line); }
 
 void save_params(const qcb_hb_params& rp) {
   std::ostringstream f;
@@ -374,7 +303,7 @@ int main(int argc, char* argv[]) {
               << std::endl;
     return 1;
   }
-  auto ex = extra_keys(argv[1]);
+  auto ex = drv::extra_keys(argv[1]);
   int precision = QCB_FP64, storage = QCB_R18, device = 0;
   if (ex.count("precision")) precision = (ex["precision"] == "fp32") ? QCB_FP32 : QCB_FP64;
   if (ex.count("storage")) storage = (ex["storage"] == "12") ? QCB_R12 : QCB_R18;

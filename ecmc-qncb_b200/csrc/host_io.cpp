@@ -118,20 +118,27 @@ static std::string trim_st(const std::string& s) {
   return s.substr(first, last - first + 1);
 }
 
-int params_load(const char* path, qcb_hb_params* p, std::string* err) {
+// key -> value of an input file, with the line rules above.
+static int read_config(const char* path, std::map<std::string, std::string>* cfg, std::string* err) {
   std::ifstream file(path);
   if (!file.is_open()) {
     *err = std::string("Can't open file ") + path;
     return QCB_ERR_IO;
   }
-  std::map<std::string, std::string> cfg;
   std::string line;
   while (std::getline(file, line)) {
     if (line.empty() || line[0] == '#') continue;
     std::istringstream is(line);
     std::string key, value;
-    if (std::getline(is, key, '=') && std::getline(is, value)) cfg[trim_st(key)] = trim_st(value);
+    if (std::getline(is, key, '=') && std::getline(is, value)) (*cfg)[trim_st(key)] = trim_st(value);
   }
+  return QCB_OK;
+}
+
+int params_load(const char* path, qcb_hb_params* p, std::string* err) {
+  std::map<std::string, std::string> cfg;
+  int r = read_config(path, &cfg, err);
+  if (r != QCB_OK) return r;
   try {
     auto geti = [&](const char* k, int& dst) {
       auto it = cfg.find(k);
@@ -176,4 +183,60 @@ int params_load(const char* path, qcb_hb_params* p, std::string* err) {
   return QCB_OK;
 }
 
+// io::load_params(const std::string&, RunParamsECB&) (src/io/io.cpp:298-341): the same line
+// rules; ECMC keys are param_theta_sample, param_theta_refresh_site, param_theta_refresh_R,
+// poisson ("true" only), epsilon_set.
+int ecmc_params_load(const char* path, qcb_ecmc_run_params* p, std::string* err) {
+  std::map<std::string, std::string> cfg;
+  int r = read_config(path, &cfg, err);
+  if (r != QCB_OK) return r;
+  try {
+    auto geti = [&](const char* k, int& dst) {
+      auto it = cfg.find(k);
+      if (it != cfg.end()) dst = std::stoi(it->second);
+    };
+    auto getd = [&](const char* k, double& dst) {
+      auto it = cfg.find(k);
+      if (it != cfg.end()) dst = std::stod(it->second);
+    };
+    auto getb = [&](const char* k, int& dst) {
+      auto it = cfg.find(k);
+      if (it != cfg.end()) dst = (it->second == "true") ? 1 : 0;
+    };
+    auto gets = [&](const char* k, char* dst, size_t cap) {
+      auto it = cfg.find(k);
+      if (it != cfg.end()) {
+        strncpy(dst, it->second.c_str(), cap - 1);
+        dst[cap - 1] = 0;
+      }
+    };
+    geti("L_core", p->L_core);
+    geti("n_core_dims", p->n_core_dims);
+    getb("cold_start", p->cold_start);
+    geti("seed", p->seed);
+    geti("N_shift", p->N_shift);
+    getd("beta", p->ecmc.beta);
+    getd("param_theta_sample", p->ecmc.theta_sample);
+    getd("param_theta_refresh_site", p->ecmc.theta_refresh_site);
+    getd("param_theta_refresh_R", p->ecmc.theta_refresh_R);
+    getb("poisson", p->ecmc.poisson);
+    getd("epsilon_set", p->ecmc.epsilon_set);
+    geti("N_shift_plaquette", p->N_shift_plaquette);
+    geti("N_shift_therm", p->N_therm);
+    getb("topo", p->topo);
+    geti("N_shift_topo", p->N_shift_topo);
+    geti("N_steps_gf", p->N_steps_gf);
+    geti("N_rk_steps", p->N_rk_steps);
+    gets("run_name", p->run_name, sizeof p->run_name);
+    gets("run_dir", p->run_dir, sizeof p->run_dir);
+    geti("save_each_shifts", p->save_each_shifts);
+    p->ecmc.l_core = p->L_core;
+  } catch (const std::exception& e) {
+    *err = std::string("Error reading input : ") + e.what();
+    return QCB_ERR_FORMAT;
+  }
+  return QCB_OK;
+}
+
 }  // namespace qcb
+

@@ -24,7 +24,8 @@ int lime_find(FILE* fp, const char* type, uint64_t* offset, uint64_t* nbytes, st
 // ILDG "ildg-format" XML record body (reference: generate_ildg_xml, src/io/ildg.cpp:13-22).
 std::string ildg_xml(const int dims[4]);
 
-// Input-file parser (semantics in host_io.cpp); p must hold the defaults on entry.
+// Input-file parsers (semantics in host_io.cpp); p must hold the defaults on entry.
 int params_load(const char* path, qcb_hb_params* p, std::string* err);
+int ecmc_params_load(const char* path, qcb_ecmc_run_params* p, std::string* err);
 
 }  // namespace qcb

@@ -116,15 +116,6 @@ __device__ __forceinline__ void st(double2* links, uint32_t s, int mu, const M& 
   for (int c = 0; c < 9; ++c) q[c] = make_double2(u.e[c / 3][c % 3].re, u.e[c / 3][c % 3].im);
 }
 
-__device__ __forceinline__ M adj(const M& a) {
-  M r;
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) r.e[i][j] = conj(a.e[j][i]);
-  return r;
-}
-
 // The block of one chain: local coordinates lc (in [-1, l] for every link a chain at an
 // active link reads; -1 and l are the neighbouring blocks' faces, the reference's halo) sit
 // at stored site b_d l + lc_d - cum_d (mod L_d), with base_d = b_d l - cum_d in
@@ -224,12 +215,45 @@ __device__ __forceinline__ double ds_of(const M& P, const Herm& q) {
   return s;
 }
 
-// dS of lift candidate i under Q (not inlined: keeps the lift's link loads and products out
-// of the event loop's register budget).
-__device__ __noinline__ double lift_ds(int i, bool fwd, const double2* L, uint32_t s0, uint32_t s1, uint32_t s2,
-                                       uint32_t s3, int mu, int nu, Herm q);
-
 __device__ __forceinline__ int dsign(double x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
+
+// ---- row streaming: a product is formed one row at a time, so that only one full
+// matrix and a row or two are held in registers (a full FP64 SU(3) matrix is 36 registers)
+__device__ __forceinline__ void ld_row(const double2* L, uint32_t s, int mu, int row, Z out[3]) {
+  const double2* q = L + ((size_t)s * 4 + (size_t)mu) * 9 + 3 * row;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double2 v = q[c];
+    out[c] = mk(v.x, v.y);
+  }
+}
+// out_c = sum_a v_a M_ac
+__device__ __forceinline__ void vmul(const Z v[3], const M& m, Z out[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out[c] = v[0] * m.e[0][c] + v[1] * m.e[1][c] + v[2] * m.e[2][c];
+}
+// out_c = sum_a v_a conj(M_ca)  (v times M^+)
+__device__ __forceinline__ void vmul_a(const Z v[3], const M& m, Z out[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out[c] = v[0] * conj(m.e[c][0]) + v[1] * conj(m.e[c][1]) + v[2] * conj(m.e[c][2]);
+}
+// Q_km of the Hermitian Q
+__device__ __forceinline__ Z qel(const Herm& q, int k, int m) {
+  if (k == m) return mk(q.d[k], 0.0);
+  const int i = (k + m == 1) ? 0 : (k + m == 2 ? 1 : 2);
+  return k < m ? q.o[i] : conj(q.o[i]);
+}
+// row m's share of Im tr(X Q): sum_k Im(X_mk Q_km)
+__device__ __forceinline__ double im_row_q(const Z r[3], const Herm& q, int m) {
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const Z a = qel(q, k, m);
+    s += r[k].re * a.im + r[k].im * a.re;
+  }
+  return s;
+}
+
 
 // Link i of lift plaquette (fwd, nu) at local coordinates out, direction returned
 // (GeometryCB.cpp:58-90): 0 = (x, mu); forward 1 = (x+mu, nu), 2 = (x+nu, mu), 3 = (x, nu);
@@ -243,26 +267,97 @@ __device__ __forceinline__ int lift_link(int i, bool fwd, const int lc[4], int m
   }
 }
 
-// The plaquette of lift candidate i, read from link i (lift_improved_fast,
-// ecmc_mpi_cb.cpp:293-316), links loaded where they are used: forward P0 = U0 U1 (U3 U2)^+,
-// P1 = U1 (U3 U2)^+ U0, P2 = U2 (U0 U1)^+ U3 (P3 = P0^+); backward T = U0 (U2 U1)^+,
-// P0 = T U3, P1 = U1 U0^+ U3^+ U2, P3 = U3 T (P2 = P3^+).  s0..s3 are the links' sites.
-__device__ __forceinline__ M lift_plaquette(int i, bool fwd, const double2* L, uint32_t s0, uint32_t s1, uint32_t s2,
-                                            uint32_t s3, int mu, int nu) {
-  if (fwd) {
-    if (i == 0) return mul_na(mul_nn(ld(L, s0, mu), ld(L, s1, nu)), mul_nn(ld(L, s3, nu), ld(L, s2, mu)));
-    if (i == 1) return mul_nn(mul_na(ld(L, s1, nu), mul_nn(ld(L, s3, nu), ld(L, s2, mu))), ld(L, s0, mu));
-    return mul_nn(mul_na(ld(L, s2, mu), mul_nn(ld(L, s0, mu), ld(L, s1, nu))), ld(L, s3, nu));
-  }
-  if (i == 1) return mul_nn(mul_na(mul_na(ld(L, s1, nu), ld(L, s0, mu)), ld(L, s3, nu)), ld(L, s2, mu));
-  const M Tb = mul_na(ld(L, s0, mu), mul_nn(ld(L, s2, mu), ld(L, s1, nu)));
-  if (i == 0) return mul_nn(Tb, ld(L, s3, nu));
-  return mul_nn(ld(L, s3, nu), Tb);
+// U or U^+ by a flag, element by element (no branch).
+__device__ __forceinline__ M cdag(const M& u, bool dag) {
+  M r;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const Z a = u.e[i][j], b = u.e[j][i];
+      r.e[i][j] = dag ? mk(b.re, -b.im) : a;
+    }
+  return r;
 }
 
-__device__ __noinline__ double lift_ds(int i, bool fwd, const double2* L, uint32_t s0, uint32_t s1, uint32_t s2,
-                                       uint32_t s3, int mu, int nu, Herm q) {
-  return ds_of(lift_plaquette(i, fwd, L, s0, s1, s2, s3, mu, nu), q);
+// Q = R diag(1, -1, 0) R^dagger from columns 0 and 1 of R.
+__device__ __forceinline__ Herm ds_matrix_cols(const Z c0[3], const Z c1[3]) {
+  Herm q;
+#pragma unroll
+  for (int m = 0; m < 3; ++m)
+    q.d[m] = c0[m].re * c0[m].re + c0[m].im * c0[m].im - c1[m].re * c1[m].re - c1[m].im * c1[m].im;
+  q.o[0] = c0[0] * conj(c0[1]) - c1[0] * conj(c1[1]);
+  q.o[1] = c0[0] * conj(c0[2]) - c1[0] * conj(c1[2]);
+  q.o[2] = c0[1] * conj(c0[2]) - c1[1] * conj(c1[2]);
+  return q;
+}
+
+// The lift's plaquette (lift_improved_fast, ecmc_mpi_cb.cpp:277-337) as F0 F1 F2 F3 with
+// F0 = U0, F2 = U2^+ and, forward, F1 = U1, F3 = U3^+ or, backward, F1 = U1^+, F3 = U3.  The
+// P of each link of the reference is a cyclic rotation rot_s = F_s F_s+1 F_s+2 F_s+3 or the
+// adjoint of one, so every dS is +-Im tr(Q rot_s) for s = 0, 3 and X (1 forward, 2 backward):
+// forward P0 = rot0, P1 = rot1, P2 = rot3^+, P3 = rot0^+; backward P0 = rot0, P1 = rot2^+,
+// P2 = rot3^+, P3 = rot3.  The traces against the current Q and the proposal's Qn come out
+// of seven SU(3) products with no branch on the plaquette's orientation.  Not inlined: the
+// products would otherwise share the event loop's register budget.
+struct LiftTraces {
+  double t0, t3, tx, n0, n3, nx;
+};
+__device__ __noinline__ LiftTraces lift_traces(const double2* L, uint32_t x, uint32_t s1, uint32_t s2, uint32_t s3,
+                                               int mu, int nu, bool fwd, Herm q, Herm qn) {
+  LiftTraces t = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  const M B = mul_an(ld(L, s2, mu), cdag(ld(L, s3, nu), fwd));  // F2 F3
+  const M F1 = cdag(ld(L, s1, nu), !fwd);
+  // rot0 = F0 F1 (F2 F3), by rows of F0
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    Z u[3], a[3], r[3];
+    ld_row(L, x, mu, m, u);
+    vmul(u, F1, a);
+    vmul(a, B, r);
+    t.t0 += im_row_q(r, q, m);
+    t.n0 += im_row_q(r, qn, m);
+  }
+  if (fwd) {  // rot1 = F1 (F2 F3) F0, by rows of F1
+    const M U0 = ld(L, x, mu);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      Z a[3], r[3];
+      vmul(F1.e[m], B, a);
+      vmul(a, U0, r);
+      t.tx += im_row_q(r, q, m);
+      t.nx += im_row_q(r, qn, m);
+    }
+  } else {  // rot2 = (F2 F3)(F0 F1), by rows of F2 F3
+    const M A = mul_nn(ld(L, x, mu), F1);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      Z r[3];
+      vmul(B.e[m], A, r);
+      t.tx += im_row_q(r, q, m);
+      t.nx += im_row_q(r, qn, m);
+    }
+  }
+  // rot3 = F3 (F0 F1) F2, by rows of F3 (row m of U3^+ is the conjugated column m of U3)
+  {
+    const M A = mul_nn(ld(L, x, mu), F1);
+    const M U2 = ld(L, s2, mu);
+    const double2* u3 = L + ((size_t)s3 * 4 + (size_t)nu) * 9;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      Z f[3], a[3], r[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double2 v = u3[fwd ? 3 * c + m : 3 * m + c];
+        f[c] = mk(v.x, fwd ? -v.y : v.y);
+      }
+      vmul(f, A, a);
+      vmul_a(a, U2, r);
+      t.t3 += im_row_q(r, q, m);
+      t.n3 += im_row_q(r, qn, m);
+    }
+  }
+  return t;
 }
 
 // su2_quaternion_to_su3 (src/su3/utils.cpp:33-45) of (x0, x1, x2, x3) in subgroup (i, j).
@@ -388,13 +483,17 @@ __global__ void __launch_bounds__(64) k_ecmc_sample(EcmcLaunch a) {
     const uint32_t x = blk.site(lc);
     // rows 0 and 1 of T = R^dagger U: all the reject angles need
     M T;
-    {
-      const M U = ld(links, x, mu);
 #pragma unroll
-      for (int i = 0; i < 2; ++i)
+    for (int j2 = 0; j2 < 3; ++j2) T.e[0][j2] = T.e[1][j2] = mk(0.0, 0.0);
 #pragma unroll
-        for (int j2 = 0; j2 < 3; ++j2)
-          T.e[i][j2] = conj(R.e[0][i]) * U.e[0][j2] + conj(R.e[1][i]) * U.e[1][j2] + conj(R.e[2][i]) * U.e[2][j2];
+    for (int c = 0; c < 3; ++c) {
+      Z ur[3];
+      ld_row(links, x, mu, c, ur);
+#pragma unroll
+      for (int j2 = 0; j2 < 3; ++j2) {
+        T.e[0][j2] = T.e[0][j2] + conj(R.e[c][0]) * ur[j2];
+        T.e[1][j2] = T.e[1][j2] + conj(R.e[c][1]) * ur[j2];
+      }
     }
     // compute_list_staples (ecmc_mpi_cb.cpp:12-36): for each nu != mu, forward then backward;
     // the first minimum of the six reject angles
@@ -405,38 +504,61 @@ __global__ void __launch_bounds__(64) k_ecmc_sample(EcmcLaunch a) {
       const int nu = (k >> 1) + ((k >> 1) >= mu ? 1 : 0);
       int p[4], q[4];
       Z P00 = mk(0.0, 0.0), P11 = mk(0.0, 0.0);
-      if ((k & 1) == 0) {  // U_nu(x+mu) (U_nu(x) U_mu(x+nu))^+
+      if ((k & 1) == 0) {  // S = X W^+, X = U_nu(x+mu), W = U_nu(x) U_mu(x+nu)
         shifted(lc, mu, 1, -1, 0, p);
         shifted(lc, nu, 1, -1, 0, q);
-        const M W = mul_nn(ld(links, x, nu), ld(links, blk.site(q), mu));
-        Z v0[3], v1[3];
+        // v_k = (W^+ R)_k0 and (W^+ R)_k1, by rows of W
+        Z v0[3] = {mk(0.0, 0.0), mk(0.0, 0.0), mk(0.0, 0.0)}, v1[3] = {v0[0], v0[1], v0[2]};
+        {
+          const M C = ld(links, blk.site(q), mu);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            Z b[3], w[3];
+            ld_row(links, x, nu, c, b);
+            vmul(b, C, w);
+#pragma unroll
+            for (int kk = 0; kk < 3; ++kk) {
+              v0[kk] = v0[kk] + conj(w[kk]) * R.e[c][0];
+              v1[kk] = v1[kk] + conj(w[kk]) * R.e[c][1];
+            }
+          }
+        }
+        // y_i = T_i. X, by rows of X
+        Z y0[3] = {mk(0.0, 0.0), mk(0.0, 0.0), mk(0.0, 0.0)}, y1[3] = {y0[0], y0[1], y0[2]};
+        const uint32_t sp = blk.site(p);
+#pragma unroll
+        for (int a2 = 0; a2 < 3; ++a2) {
+          Z xr[3];
+          ld_row(links, sp, nu, a2, xr);
+#pragma unroll
+          for (int kk = 0; kk < 3; ++kk) {
+            y0[kk] = y0[kk] + T.e[0][a2] * xr[kk];
+            y1[kk] = y1[kk] + T.e[1][a2] * xr[kk];
+          }
+        }
 #pragma unroll
         for (int kk = 0; kk < 3; ++kk) {
-          v0[kk] = conj(W.e[0][kk]) * R.e[0][0] + conj(W.e[1][kk]) * R.e[1][0] + conj(W.e[2][kk]) * R.e[2][0];
-          v1[kk] = conj(W.e[0][kk]) * R.e[0][1] + conj(W.e[1][kk]) * R.e[1][1] + conj(W.e[2][kk]) * R.e[2][1];
+          P00 = P00 + y0[kk] * v0[kk];
+          P11 = P11 + y1[kk] * v1[kk];
         }
-        const M X = ld(links, blk.site(p), nu);
-#pragma unroll
-        for (int kk = 0; kk < 3; ++kk) {
-          P00 = P00 + (T.e[0][0] * X.e[0][kk] + T.e[0][1] * X.e[1][kk] + T.e[0][2] * X.e[2][kk]) * v0[kk];
-          P11 = P11 + (T.e[1][0] * X.e[0][kk] + T.e[1][1] * X.e[1][kk] + T.e[1][2] * X.e[2][kk]) * v1[kk];
-        }
-      } else {  // (U_mu(x-nu) U_nu(x+mu-nu))^+ U_nu(x-nu)
+      } else {  // S = W^+ D, W = U_mu(x-nu) U_nu(x+mu-nu), D = U_nu(x-nu)
         shifted(lc, mu, 1, nu, -1, p);
         shifted(lc, nu, -1, -1, 0, q);
         const uint32_t sq = blk.site(q);
-        const M W = mul_nn(ld(links, sq, mu), ld(links, blk.site(p), nu));
-        Z y0[3], y1[3];
+        const M C = ld(links, blk.site(p), nu);
+        // P_ii = sum_k (T_i. W^+)_k (D R)_ki, by rows k of W and of D
 #pragma unroll
         for (int kk = 0; kk < 3; ++kk) {
-          y0[kk] = T.e[0][0] * conj(W.e[kk][0]) + T.e[0][1] * conj(W.e[kk][1]) + T.e[0][2] * conj(W.e[kk][2]);
-          y1[kk] = T.e[1][0] * conj(W.e[kk][0]) + T.e[1][1] * conj(W.e[kk][1]) + T.e[1][2] * conj(W.e[kk][2]);
-        }
-        const M D = ld(links, sq, nu);
-#pragma unroll
-        for (int kk = 0; kk < 3; ++kk) {
-          P00 = P00 + y0[kk] * (D.e[kk][0] * R.e[0][0] + D.e[kk][1] * R.e[1][0] + D.e[kk][2] * R.e[2][0]);
-          P11 = P11 + y1[kk] * (D.e[kk][0] * R.e[0][1] + D.e[kk][1] * R.e[1][1] + D.e[kk][2] * R.e[2][1]);
+          Z b[3], w[3], d[3];
+          ld_row(links, sq, mu, kk, b);
+          vmul(b, C, w);
+          const Z y0 = T.e[0][0] * conj(w[0]) + T.e[0][1] * conj(w[1]) + T.e[0][2] * conj(w[2]);
+          const Z y1 = T.e[1][0] * conj(w[0]) + T.e[1][1] * conj(w[1]) + T.e[1][2] * conj(w[2]);
+          ld_row(links, sq, nu, kk, d);
+          const Z z0 = d[0] * R.e[0][0] + d[1] * R.e[1][0] + d[2] * R.e[2][0];
+          const Z z1 = d[0] * R.e[0][1] + d[1] * R.e[1][1] + d[2] * R.e[2][1];
+          P00 = P00 + y0 * z0;
+          P11 = P11 + y1 * z1;
         }
       }
       const double rej = reject_from(P00, P11, a.beta, -log(g.uni()), eps);
@@ -455,18 +577,30 @@ __global__ void __launch_bounds__(64) k_ecmc_sample(EcmcLaunch a) {
       break;
     }
     const int kind = (step == d_sample) ? 0 : (step == d_site) ? 1 : (step == d_R) ? 2 : 3;
-    // update (ecmc_mpi_cb.cpp:340-356): U <- R diag(e^{i xi}, e^{-i xi}, 1) R^dagger U
+    // update (ecmc_mpi_cb.cpp:340-356): U <- R diag(e^{i xi}, e^{-i xi}, 1) R^dagger U, the
+    // rows of T = R^dagger U: 0 and 1 from above, 2 from U; written row by row
     {
       double sn, cs;
       sincos((double)eps * step, &sn, &cs);
-      const M U = ld(links, x, mu);
-      M T2 = mul_an(R, U);
+      Z t2[3] = {mk(0.0, 0.0), mk(0.0, 0.0), mk(0.0, 0.0)};
 #pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        T2.e[0][cc] = T2.e[0][cc] * mk(cs, sn);
-        T2.e[1][cc] = T2.e[1][cc] * mk(cs, -sn);
+      for (int c = 0; c < 3; ++c) {
+        Z ur[3];
+        ld_row(links, x, mu, c, ur);
+#pragma unroll
+        for (int j2 = 0; j2 < 3; ++j2) t2[j2] = t2[j2] + conj(R.e[c][2]) * ur[j2];
       }
-      st(links, x, mu, mul_nn(R, T2));
+      const Z ep = mk(cs, sn), em = mk(cs, -sn);
+      double2* q = links + ((size_t)x * 4 + (size_t)mu) * 9;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const Z r0 = R.e[i][0] * ep, r1 = R.e[i][1] * em, r2 = R.e[i][2];
+#pragma unroll
+        for (int j2 = 0; j2 < 3; ++j2) {
+          const Z v = r0 * T.e[0][j2] + r1 * T.e[1][j2] + r2 * t2[j2];
+          q[3 * i + j2] = make_double2(v.re, v.im);
+        }
+      }
       ++events;
     }
     if (kind == 0) {
@@ -505,54 +639,47 @@ __global__ void __launch_bounds__(64) k_ecmc_sample(EcmcLaunch a) {
       lift_link(3, fwd, lc, mu, nu, t4);
       const uint32_t s3 = blk.site(t4);
       const bool f3 = blk.frozen(t4, nu);
-      const Herm Q = ds_matrix(R);
-      // dS of each candidate (0 for frozen links); the adjoint pair of the plaquette (forward
-      // 0 and 3, backward 2 and 3) has opposite dS
-      double ds0, ds1, ds2, ds3;
-      if (fwd) {
-        ds0 = lift_ds(0, true, links, x, s1, s2, s3, mu, nu, Q);
-        ds1 = f1 ? 0.0 : lift_ds(1, true, links, x, s1, s2, s3, mu, nu, Q);
-        ds2 = f2 ? 0.0 : lift_ds(2, true, links, x, s1, s2, s3, mu, nu, Q);
-        ds3 = f3 ? 0.0 : -ds0;
-      } else {
-        ds0 = lift_ds(0, false, links, x, s1, s2, s3, mu, nu, Q);
-        ds1 = f1 ? 0.0 : lift_ds(1, false, links, x, s1, s2, s3, mu, nu, Q);
-        const double d3 = lift_ds(3, false, links, x, s1, s2, s3, mu, nu, Q);
-        ds3 = f3 ? 0.0 : d3;
-        ds2 = f2 ? 0.0 : -d3;
+      // selectVariable's uniform and the set index, in the reference's order, before the
+      // plaquette: the proposal R_new = S R is known in advance and its dS rides along
+      const double r = g.uni();
+      const int iset = (int)(g.uni() * (double)ECMC_SET_SIZE);
+      const double2* sq = set + (size_t)iset * 9;
+      Herm Qn;
+      {
+        Z c0[3], c1[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          const double2 s0 = sq[3 * m], s1v = sq[3 * m + 1], s2v = sq[3 * m + 2];
+          const Z a0 = mk(s0.x, s0.y), a1 = mk(s1v.x, s1v.y), a2 = mk(s2v.x, s2v.y);
+          c0[m] = a0 * R.e[0][0] + a1 * R.e[1][0] + a2 * R.e[2][0];
+          c1[m] = a0 * R.e[0][1] + a1 * R.e[1][1] + a2 * R.e[2][1];
+        }
+        Qn = ds_matrix_cols(c0, c1);
       }
+      const LiftTraces tr = lift_traces(links, x, s1, s2, s3, mu, nu, fwd, ds_matrix(R), Qn);
+      // dS of each candidate (0 for frozen links) under R and under R_new
+      const double ds0 = tr.t0, dn0 = tr.n0;
+      const double ds1 = f1 ? 0.0 : (fwd ? tr.tx : -tr.tx), dn1 = fwd ? tr.nx : -tr.nx;
+      const double ds2 = f2 ? 0.0 : -tr.t3, dn2 = -tr.n3;
+      const double ds3 = f3 ? 0.0 : (fwd ? -tr.t0 : tr.t3), dn3 = fwd ? -tr.n0 : tr.n3;
       const double a0 = fabs(ds0), a1 = fabs(ds1), a2 = fabs(ds2), a3 = fabs(ds3);
       const double sum = a0 + a1 + a2 + a3;
       const double p0 = a0 / sum, p1 = a1 / sum, p2 = a2 / sum;
       // selectVariable (ecmc_mpi_cb.cpp:252-260)
-      const double r = g.uni();
       const int idx = r < p0 ? 0 : (r < p0 + p1 ? 1 : (r < p0 + p1 + p2 ? 2 : 3));
       const double ds_old = idx == 0 ? ds0 : idx == 1 ? ds1 : idx == 2 ? ds2 : ds3;
-      const int iset = (int)(g.uni() * (double)ECMC_SET_SIZE);
-      M Rn;
-      {
-        M Sx;
-        const double2* q = set + (size_t)iset * 9;
-#pragma unroll
-        for (int cc = 0; cc < 9; ++cc) {
-          const double2 v = q[cc];
-          Sx.e[cc / 3][cc % 3] = mk(v.x, v.y);
-        }
-        Rn = mul_nn(Sx, R);
-      }
-      // P of the chosen link: the adjoint partner reuses its pair's plaquette
-      double ds_new;
-      if (fwd && idx == 3)
-        ds_new = -lift_ds(0, true, links, x, s1, s2, s3, mu, nu, ds_matrix(Rn));
-      else if (!fwd && idx == 2)
-        ds_new = -lift_ds(3, false, links, x, s1, s2, s3, mu, nu, ds_matrix(Rn));
-      else
-        ds_new = lift_ds(idx, fwd, links, x, s1, s2, s3, mu, nu, ds_matrix(Rn));
+      const double ds_new = idx == 0 ? dn0 : idx == 1 ? dn1 : idx == 2 ? dn2 : dn3;
       int new_eps = -dsign(ds_old);
       bool take = fabs(ds_old) < fabs(ds_new);
       if (!take) take = g.uni() < fabs(ds_new) / fabs(ds_old);
       if (take) {
-        R = Rn;
+        M Sx;
+#pragma unroll
+        for (int cc = 0; cc < 9; ++cc) {
+          const double2 v = sq[cc];
+          Sx.e[cc / 3][cc % 3] = mk(v.x, v.y);
+        }
+        R = mul_nn(Sx, R);
         new_eps = -dsign(ds_new);
       }
       const int nmu = lift_link(idx, fwd, lc, mu, nu, t4);

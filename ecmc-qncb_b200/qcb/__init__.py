@@ -421,6 +421,15 @@ class io:
         return p
 
     @staticmethod
+    def load_ecmc_params(path):
+        """io::load_params(file, RunParamsECB&) (src/io/io.cpp:298-341) -> EcmcRunParams."""
+        from ._lib import EcmcRunParams
+        p = EcmcRunParams()
+        check(lib().qcb_ecmc_run_params_default(C.byref(p)))
+        check(lib().qcb_ecmc_run_params_load(os.fsencode(path), C.byref(p)))
+        return p
+
+    @staticmethod
     def ildg_probe(path):
         off, n = C.c_uint64(), C.c_uint64()
         check(lib().qcb_ildg_probe(os.fsencode(path), C.byref(off), C.byref(n)))

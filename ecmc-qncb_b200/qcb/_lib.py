@@ -83,6 +83,25 @@ class EcmcParams(C.Structure):
                 ("l_core", C.c_int)]
 
 
+class EcmcRunParams(C.Structure):
+    """qcb_ecmc_run_params: RunParamsECB of the reference (src/io/params.h:27-44)."""
+    _fields_ = [("L_core", C.c_int), ("n_core_dims", C.c_int), ("cold_start", C.c_int), ("seed", C.c_int),
+                ("N_shift", C.c_int), ("ecmc", EcmcParams),
+                ("N_therm", C.c_int), ("topo", C.c_int), ("N_shift_plaquette", C.c_int), ("N_shift_topo", C.c_int),
+                ("N_steps_gf", C.c_int), ("N_rk_steps", C.c_int), ("save_each_shifts", C.c_int),
+                ("run_name", C.c_char * 256), ("run_dir", C.c_char * 1024)]
+
+    def as_dict(self) -> dict:
+        d = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            if name == "ecmc":
+                d.update({k: getattr(v, k) for k, _ in v._fields_})
+            else:
+                d[name] = v.decode() if isinstance(v, bytes) else v
+        return d
+
+
 _lib = None
 
 # name -> (restype, argtypes)
@@ -157,6 +176,8 @@ SIGNATURES = {
     "qcb_ecmc_set_chains": (C.c_int, [_vp, _vp, C.c_uint64]),
     "qcb_params_default": (C.c_int, [C.POINTER(HbParams)]),
     "qcb_params_load": (C.c_int, [C.c_char_p, C.POINTER(HbParams)]),
+    "qcb_ecmc_run_params_default": (C.c_int, [C.POINTER(EcmcRunParams)]),
+    "qcb_ecmc_run_params_load": (C.c_int, [C.c_char_p, C.POINTER(EcmcRunParams)]),
 }
 
 

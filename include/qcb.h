@@ -390,6 +390,22 @@ typedef struct qcb_hb_params {
 int qcb_params_default(qcb_hb_params* p);
 int qcb_params_load(const char* path, qcb_hb_params* p);
 
+/* io::load_params(..., RunParamsECB&) (src/io/io.cpp:298-341) with the defaults of
+ * src/io/params.h:9-44, for the event-chain driver.  Same line rules as qcb_params_load;
+ * keys L_core, n_core_dims, cold_start, seed, N_shift, beta, param_theta_sample,
+ * param_theta_refresh_site, param_theta_refresh_R, poisson, epsilon_set, N_shift_plaquette,
+ * N_shift_therm, topo, N_shift_topo, N_steps_gf, N_rk_steps, run_name, run_dir,
+ * save_each_shifts.  ecmc.l_core is set to L_core.  Host-only. */
+typedef struct qcb_ecmc_run_params {
+  int L_core, n_core_dims, cold_start, seed, N_shift;
+  qcb_ecmc_params ecmc;
+  int N_therm, topo, N_shift_plaquette, N_shift_topo, N_steps_gf, N_rk_steps, save_each_shifts;
+  char run_name[256];
+  char run_dir[1024];
+} qcb_ecmc_run_params;
+int qcb_ecmc_run_params_default(qcb_ecmc_run_params* p);
+int qcb_ecmc_run_params_load(const char* path, qcb_ecmc_run_params* p);
+
 #ifdef __cplusplus
 }
 #endif

@@ -173,3 +173,29 @@ def test_driver_rejects_bad_input(tmp_path):
     bad.write_text("L_core = 4\nschedule = lexicographic\n")
     r = subprocess.run([str(driver), str(bad)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "schedule must be" in r.stderr
+
+
+def test_ecmc_params_parse_reference_example(tmp_path):
+    """The reference's inputs/ecold6.txt keys (io.cpp:298-341); unset keys keep the
+    RunParamsECB / ECMCParams defaults (params.h:9-44)."""
+    text = ("#Lattice params\nL_core=4\nn_core_dims=2\ncold_start=true\n\n#Run params\nseed=12345\n"
+            "N_shift_therm = 10\nN_shift=20\n\n#ECMC params\nbeta=6.0\nparam_theta_sample=1000\n"
+            "param_theta_refresh_site=500\nparam_theta_refresh_R=3.3\npoisson=false\nepsilon_set=0.15\n\n"
+            "#Plaquette params\nN_shift_plaquette = 2\n\n#Topo params\ntopo = false\nN_shift_topo = 25\n"
+            "N_steps_gf = 10\nN_rk_steps = 40\n\n#Save params\nrun_name = ecold58e\nrun_dir = data\n"
+            "save_each_shifts = 2000\n")
+    p = tmp_path / "ecold6.txt"
+    p.write_text(text)
+    got = qcb.io.load_ecmc_params(p).as_dict()
+    want = dict(L_core=4, n_core_dims=2, cold_start=1, seed=12345, N_shift=20, beta=6.0, theta_sample=1000.0,
+                theta_refresh_site=500.0, theta_refresh_R=3.3, poisson=0, epsilon_set=0.15, l_core=4, N_therm=10,
+                topo=0, N_shift_plaquette=2, N_shift_topo=25, N_steps_gf=10, N_rk_steps=40, run_name="ecold58e",
+                run_dir="data", save_each_shifts=2000)
+    assert got == want
+    p.write_text("poisson = true\nL_core = 5\n")
+    got = qcb.io.load_ecmc_params(p).as_dict()
+    assert got["poisson"] == 1 and got["l_core"] == 5 and got["theta_sample"] == 100.0 and got["N_therm"] == 100
+    p.write_text("param_theta_sample = abc\n")
+    with pytest.raises(qcb.QcbError) as e:
+        qcb.io.load_ecmc_params(p)
+    assert e.value.code == 4
