@@ -416,12 +416,6 @@ def batch_section(ctx, lib, stream):
 
 
 ECMC_L, ECMC_LCORE, ECMC_THETA = 64, 4, 100.0
-# FP64 operations of one ECMC event (a lift; refresh events are rarer and cheaper), counted
-# from the kernel's source: six staples (one SU(3) product, two projected columns and two
-# projected rows: 69 complex multiply-adds each), the update (two SU(3) products), the lift
-# (seven SU(3) products for three plaquettes, the set element times R, dS traces) and the
-# reject-angle solves (log, hypot, atan2, asin, a division: about 120 operations each).
-ECMC_FLOP_PER_EVENT = 8 * (6 * 69 + 2 * 27 + 8 * 27 + 6 * 9) + 6 * 120
 FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64 (non-tensor), NVIDIA's nominal figure; not measured here
 
 
@@ -497,7 +491,9 @@ def ecmc_section(ctx, steps=5, warmup=3, cpu_budget_s=8.0, cpu=True):
         plaq = qcb.observables.mean_plaquette_global(f)
     e2e_s = (time.perf_counter() - t) / steps
     e_ev, _, _ = ch.counters(reset=True)
-    flop = ECMC_FLOP_PER_EVENT * rate / 1e12
+    traffic = ncu_traffic()
+    flop_per_event = traffic.get("ecmc_fp64_flop_per_event")
+    flop = flop_per_event * rate / 1e12 if flop_per_event else None
     out = {"metric": "ECMC events/s (one link update each)", "value": rate, "unit": "events/s",
            "workload": f"{ECMC_L}^4 fp64, {ch.n_chains} chains of {ECMC_LCORE}^4 blocks, beta={BETA}, theta_sample="
                        f"{ECMC_THETA:g}, refresh 50/15, epsilon_set 0.15",
@@ -507,9 +503,11 @@ def ecmc_section(ctx, steps=5, warmup=3, cpu_budget_s=8.0, cpu=True):
            "e2e": {"value": e_ev / (e2e_s * steps), "unit": "events/s", "s_per_step": e2e_s,
                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8,
                    "step": "random translation + qcb_ecmc_sample + qcb_plaquette to host, links resident"},
-           "roofline": {"bound": "fp64", "achieved": flop, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
-                        "frac": flop / FP64_NOMINAL_TFLOPS, "peak_kind": "nominal (no FP64 peak is measured)",
-                        "flop_per_event": ECMC_FLOP_PER_EVENT}}
+           "roofline": {"bound": "fp64 (latency and register bound in practice)", "achieved": flop,
+                        "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                        "frac": flop / FP64_NOMINAL_TFLOPS if flop else None,
+                        "peak_kind": "nominal (no FP64 peak is measured)", "flop_per_event": flop_per_event,
+                        "dram_bytes_per_event_ncu": traffic.get("ecmc_dram_bytes_per_event")}}
     ch.close()
     f.close()
     if cpu:
@@ -520,6 +518,26 @@ def ecmc_section(ctx, steps=5, warmup=3, cpu_budget_s=8.0, cpu=True):
                                "cores": cores, "kind": "port",
                                "sample": f"{cores} processes x the oracle's 16 chains on an 8^4 lattice of 4^4 "
                                          f"blocks, theta_sample {ECMC_THETA:g} calls for {cpu_budget_s:g} s"}
+    return out
+
+
+def ecmc_profile_case(ctx):
+    """The small case an ncu capture of k_ecmc_sample runs on (a few GB on the device): a 42^4
+    FP64 lattice as 14^4 blocks of 3^4 (38416 chains, a full wave of resident chains), Haar
+    hot start + 5 heatbath sweeps, two sample calls (capture the second: -s 1 -c 1)."""
+    import qcb
+
+    f = qcb.GaugeField(ctx, (42,) * 4, "fp64", 18)
+    f.hot_start(1)
+    qcb._lib.check(qcb._lib.lib().qcb_heatbath(f.h, BETA, 5, 1, 3, 0))
+    ch = qcb.EventChains(f, qcb.ecmc.params(beta=BETA, theta_sample=ECMC_THETA, l_core=3), 7)
+    ch.sample((0, 1, 2, 0))
+    ch.counters(reset=True)
+    ch.sample((1, 1, 0, 2))
+    events, lifts, revs = ch.counters(reset=True)
+    out = {"case": "ecmc 42^4 l_core 3", "chains": ch.n_chains, "events_second_call": events, "lifts": lifts}
+    ch.close()
+    f.close()
     return out
 
 
@@ -848,7 +866,11 @@ def main():
             import qcb
 
             ctx = qcb.Context(0)
-            print(json.dumps(ecmc_section(ctx, steps=args.steps, warmup=args.warmup, cpu=not args.no_cpu_baseline)))
+            if args.profile:
+                print(json.dumps(ecmc_profile_case(ctx)))
+            else:
+                print(json.dumps(ecmc_section(ctx, steps=args.steps, warmup=args.warmup,
+                                              cpu=not args.no_cpu_baseline)))
             ctx.close()
         return 0
     dist = replicas.init("nccl", timeout_s=300)

@@ -37,19 +37,22 @@ __device__ __forceinline__ double u53(uint32_t lo, uint32_t hi) {
   return ((double)x + 0.5) * 1.1102230246251565e-16;
 }
 
+// The k-th uniform of chain `chain` (one copy of the Philox rounds in the kernel: the
+// generator has two dozen call sites, and inlining each one overflowed the instruction cache).
+__device__ __noinline__ double chain_uniform(uint32_t chain, uint32_t k0, uint32_t k1, uint64_t k) {
+  u32x4 c;
+  c.v[0] = (uint32_t)k;
+  c.v[1] = (uint32_t)(k >> 32);
+  c.v[2] = chain;
+  c.v[3] = ECMC_CHAIN;
+  const u32x4 r = philox4x32_10(c, k0, k1);
+  return u53(r.v[0], r.v[1]);
+}
+
 struct Stream {
   uint32_t chain, k0, k1;
   uint64_t n;
-  __device__ __forceinline__ double uni() {
-    u32x4 c;
-    c.v[0] = (uint32_t)n;
-    c.v[1] = (uint32_t)(n >> 32);
-    c.v[2] = chain;
-    c.v[3] = ECMC_CHAIN;
-    ++n;
-    const u32x4 r = philox4x32_10(c, k0, k1);
-    return u53(r.v[0], r.v[1]);
-  }
+  __device__ __forceinline__ double uni() { return chain_uniform(chain, k0, k1, n++); }
 };
 
 // SU(3) from 12 standard normals: rows 0, 1 complex Gaussian, Gram-Schmidt, row 2 =
@@ -84,8 +87,9 @@ __device__ M haar_from_normals(const double n[12]) {
   return u;
 }
 
-// random_su3 (src/su3/utils.cpp:13-30), redrawn: Haar SU(3) from 6 Box-Muller pairs.
-__device__ M haar(Stream& g) {
+// random_su3 (src/su3/utils.cpp:13-30), redrawn: Haar SU(3) from 6 Box-Muller pairs (not
+// inlined: it runs at initialisation and at R refreshes only).
+__device__ __noinline__ M haar(Stream& g) {
   double n[12];
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
@@ -108,12 +112,6 @@ __device__ __forceinline__ M ld(const double2* links, uint32_t s, int mu) {
     u.e[c / 3][c % 3] = mk(v.x, v.y);
   }
   return u;
-}
-
-__device__ __forceinline__ void st(double2* links, uint32_t s, int mu, const M& u) {
-  double2* q = links + ((size_t)s * 4 + (size_t)mu) * 9;
-#pragma unroll
-  for (int c = 0; c < 9; ++c) q[c] = make_double2(u.e[c / 3][c % 3].re, u.e[c / 3][c % 3].im);
 }
 
 // The block of one chain: local coordinates lc (in [-1, l] for every link a chain at an
@@ -201,20 +199,6 @@ __device__ __forceinline__ Herm ds_matrix(const M& R) {
   q.o[2] = R.e[1][0] * conj(R.e[2][0]) - R.e[1][1] * conj(R.e[2][1]);
   return q;
 }
-// Im tr(P Q) = sum_km Im(P_km Q_mk)
-__device__ __forceinline__ double ds_of(const M& P, const Herm& q) {
-  double s = P.e[0][0].im * q.d[0] + P.e[1][1].im * q.d[1] + P.e[2][2].im * q.d[2];
-  // P_01 Q_10 + P_10 Q_01 with Q_10 = conj(Q_01), and likewise for (0,2), (1,2)
-  const int a[3] = {0, 0, 1}, b[3] = {1, 2, 2};
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const Z pab = P.e[a[k]][b[k]], pba = P.e[b[k]][a[k]], o = q.o[k];
-    s += pab.re * (-o.im) + pab.im * o.re;  // Im(P_ab conj(o))
-    s += pba.re * o.im + pba.im * o.re;     // Im(P_ba o)
-  }
-  return s;
-}
-
 __device__ __forceinline__ int dsign(double x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
 
 // ---- row streaming: a product is formed one row at a time, so that only one full
@@ -297,9 +281,9 @@ __device__ __forceinline__ Herm ds_matrix_cols(const Z c0[3], const Z c1[3]) {
 // P of each link of the reference is a cyclic rotation rot_s = F_s F_s+1 F_s+2 F_s+3 or the
 // adjoint of one, so every dS is +-Im tr(Q rot_s) for s = 0, 3 and X (1 forward, 2 backward):
 // forward P0 = rot0, P1 = rot1, P2 = rot3^+, P3 = rot0^+; backward P0 = rot0, P1 = rot2^+,
-// P2 = rot3^+, P3 = rot3.  The traces against the current Q and the proposal's Qn come out
-// of seven SU(3) products with no branch on the plaquette's orientation.  Not inlined: the
-// products would otherwise share the event loop's register budget.
+// P2 = rot3^+, P3 = rot3.  The traces against the current Q and the proposal's Qn take
+// seven SU(3) products, row-streamed; only rot_X depends on the orientation.  Not inlined:
+// the products would otherwise share the event loop's register budget.
 struct LiftTraces {
   double t0, t3, tx, n0, n3, nx;
 };
