@@ -199,3 +199,21 @@ def test_ecmc_params_parse_reference_example(tmp_path):
     with pytest.raises(qcb.QcbError) as e:
         qcb.io.load_ecmc_params(p)
     assert e.value.code == 4
+
+
+def test_ecmc_driver_rejects_bad_input(tmp_path):
+    """The event-chain driver reports input errors before touching the GPU."""
+    import subprocess
+
+    driver = ROOT / "ecmc-qncb_b200" / "bin" / "gauge_ecmc_ncb"
+    if not driver.exists():
+        subprocess.run([sys.executable, str(ROOT / "ecmc-qncb_b200" / "build.py")], check=True)
+    bad = tmp_path / "bad.txt"
+    bad.write_text("param_theta_sample = many\n")
+    r = subprocess.run([str(driver), str(bad)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "Error reading input" in r.stderr
+    bad.write_text("L_core = 2\n")
+    r = subprocess.run([str(driver), str(bad)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "L_core must be at least 3" in r.stderr
+    r = subprocess.run([str(driver)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "Usage" in r.stderr
