@@ -98,22 +98,23 @@ def test_frozen_links_bit_identical(ctx):
     f.close()
 
 
-def test_fp32_storage_tracks_fp64(ctx):
+@pytest.mark.parametrize("precision,storage,tol", [("fp32", 12, 1e-5), ("fp64", 12, 1e-9), ("fp32", 18, 1e-5)])
+def test_other_storages_track_the_oracle(ctx, precision, storage, tol):
+    """The chains compute in FP64 on the unpacked links whatever the storage: the same events
+    as the oracle from the stored (rounded or 12-real) start, links to the storage's rounding."""
     dims = (8, 8, 8, 8)
     u = orc.hot_philox(dims, 8)
-    f = qcb.GaugeField(ctx, dims, "fp32", 12)
+    f = qcb.GaugeField(ctx, dims, precision, storage)
     f.set_links(u)
+    start = f.get_links()
     ch = qcb.EventChains(f, BASE, 9)
     ch.sample((1, 1, 1, 1))
-    # the chains see the FP32-rounded start, so compare with the oracle from the same start
-    start = qcb.GaugeField(ctx, dims, "fp32", 12)
-    start.set_links(u)
-    u32 = start.get_links()
-    ref_u, ref_c = orc.ecmc_sample(u32, dims, BASE, 9, 0, (1, 1, 1, 1), orc.ecmc_chains(dims, 4))
+    ref_u, ref_c = orc.ecmc_sample(start, dims, BASE, 9, 0, (1, 1, 1, 1), orc.ecmc_chains(dims, 4))
     rec, _ = ch.chains()
     assert np.array_equal(rec["events"], ref_c["events"])
-    assert np.abs(f.get_links() - ref_u).max() < 1e-5
-    for o in (ch, f, start):
+    assert np.array_equal(rec["draws"], ref_c["draws"])
+    assert np.abs(f.get_links() - ref_u).max() < tol
+    for o in (ch, f):
         o.close()
 
 
