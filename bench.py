@@ -420,28 +420,24 @@ FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64 (non-tensor), NVIDIA's nominal figure; n
 
 
 def _ecmc_cpu_worker(args):
-    """One host core: the oracle's chains on an 8^4 lattice of 4^4 blocks (16 chains, as the
-    reference's 16 ranks of inputs/ecold6.txt), calls of theta_sample = 100 until `budget` s."""
+    """One host core as one rank of the reference: the oracle's restatement of
+    sample_persistant with the reference's own generator (std::mt19937_64, std::
+    distributions, the rank's set regenerated per call) on a 4^4 block with frozen faces,
+    random_shift + one sample call per shift (theta_sample 100), for `budget` seconds."""
     seed, budget = args
     sys.path.insert(0, str(ROOT / "oracle"))
-    import numpy as np
-
     import oracle
 
-    dims = (8, 8, 8, 8)
     p = dict(beta=BETA, theta_sample=ECMC_THETA, theta_refresh_site=50.0, theta_refresh_R=15.0, epsilon_set=0.15,
-             poisson=0, l_core=4)
-    u, _ = oracle.heatbath_cb(oracle.hot_philox(dims, seed), dims, BETA, 20, 1, seed, 0)
-    ch = oracle.ecmc_chains(dims, 4)
-    rng = np.random.default_rng(seed)
-    cum = np.zeros(4, int)
+             poisson=0)
+    run = oracle.EcmcRefRun(ECMC_LCORE, seed, False, p)
+    run.run(5)
+    events0 = run.run(0)[1][0]
     t = time.perf_counter()
-    call = 0
+    events = events0
     while time.perf_counter() - t < budget:
-        cum = (cum + rng.integers(0, 4, 4)) % 8
-        u, ch = oracle.ecmc_sample(u, dims, p, seed, call, cum, ch)
-        call += 1
-    return int(ch["events"].sum()), time.perf_counter() - t
+        events = run.run(20)[1][0]
+    return events - events0, time.perf_counter() - t
 
 
 def ecmc_section(ctx, steps=5, warmup=3, cpu_budget_s=8.0, cpu=True):
@@ -516,8 +512,9 @@ def ecmc_section(ctx, steps=5, warmup=3, cpu_budget_s=8.0, cpu=True):
             res = pool.map(_ecmc_cpu_worker, [(500 + r, cpu_budget_s) for r in range(cores)])
         out["cpu_baseline"] = {"value": sum(r[0] for r in res) / max(r[1] for r in res), "unit": "events/s",
                                "cores": cores, "kind": "port",
-                               "sample": f"{cores} processes x the oracle's 16 chains on an 8^4 lattice of 4^4 "
-                                         f"blocks, theta_sample {ECMC_THETA:g} calls for {cpu_budget_s:g} s"}
+                               "sample": f"{cores} processes, each one rank of the reference (one chain on a "
+                                         f"{ECMC_LCORE}^4 block, the reference's std::mt19937_64 generator and "
+                                         f"per-call set), theta_sample {ECMC_THETA:g} calls for {cpu_budget_s:g} s"}
     return out
 
 

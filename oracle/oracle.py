@@ -66,6 +66,12 @@ def lib():
         L.orc_ecmc_compute_ds.argtypes = [dp, dp, dp]
         L.orc_ecmc_set.argtypes = [C.c_double, C.c_uint64, C.c_uint64, dp]
         L.orc_ecmc_sample.argtypes = [dp, ip, dp, ip, C.c_uint64, C.c_uint64, ip, C.c_void_p]
+        L.orc_ecmc_ref_create.argtypes = [C.c_int, C.c_int, C.c_int, dp, ip]
+        L.orc_ecmc_ref_create.restype = C.c_void_p
+        L.orc_ecmc_ref_destroy.argtypes = [C.c_void_p]
+        L.orc_ecmc_ref_run.argtypes = [C.c_void_p, C.c_int, dp, C.POINTER(C.c_uint64)]
+        L.orc_ecmc_ref_get_links.argtypes = [C.c_void_p, dp]
+        L.orc_ecmc_ref_set_links.argtypes = [C.c_void_p, dp]
         _lib = L
     return _lib
 
@@ -396,3 +402,38 @@ def ecmc_sample(u, dims, params: dict, seed, call, cum, chains):
     if rc:
         raise ValueError("l_core must be >= 3 and divide every extent")
     return u, ch
+
+
+class EcmcRefRun:
+    """generate_ecmc_cb on one rank with the reference's own generator (std::mt19937_64,
+    std:: distributions, Householder random_su3, the rank's set regenerated per call and every
+    10000 lifts): an L^4 lattice as one block with frozen faces, moved by random_shift before
+    each sample_persistant call."""
+
+    def __init__(self, L: int, seed: int, cold_start: bool, params: dict):
+        dp = np.array([params["beta"], params["theta_sample"], params["theta_refresh_site"],
+                       params["theta_refresh_R"], params["epsilon_set"]], np.float64)
+        ip = (C.c_int * 2)(int(params.get("poisson", 0)), int(L))
+        self.L = L
+        self.h = lib().orc_ecmc_ref_create(L, seed, 1 if cold_start else 0, _dp(dp), ip)
+
+    def run(self, n_shift: int):
+        """n_shift shifts; returns (plaquette after each, (events, lifts, same-site lifts))."""
+        plaq = np.zeros(n_shift)
+        c = (C.c_uint64 * 3)()
+        lib().orc_ecmc_ref_run(self.h, n_shift, _dp(plaq), c)
+        return plaq, (int(c[0]), int(c[1]), int(c[2]))
+
+    def links(self) -> np.ndarray:
+        u = np.zeros(shape((self.L,) * 4), np.complex128)
+        lib().orc_ecmc_ref_get_links(self.h, _dp(u))
+        return u
+
+    def set_links(self, u) -> None:
+        u = np.ascontiguousarray(u, np.complex128)
+        lib().orc_ecmc_ref_set_links(self.h, _dp(u))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_ecmc_ref_destroy(self.h)
+            self.h = None

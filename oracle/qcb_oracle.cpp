@@ -734,34 +734,53 @@ static void shifted(const int a[4], int d1, int s1, int d2, int s2, int out[4]) 
   if (d2 >= 0) out[d2] += s2;
 }
 
+// The random draws of one chain, two policies.  LibDraws: the library's counter-based stream
+// (Philox, the call's shared set).  RefDraws (below): the reference's std::mt19937_64 with
+// its std:: distributions and its own set, regenerated as the reference does.
+struct LibDraws {
+  EcmcStream g;
+  const std::vector<M3>* set;
+  int l;
+  // random_site (ecmc_mpi_cb.cpp:359-367): local coordinates 1 .. l-2 (padded 2 .. L-1)
+  void site(int lc[4]) {
+    for (int d = 0; d < 4; ++d) lc[d] = 1 + (int)(g.uni() * (double)(l - 2));
+  }
+  int dir() { return (int)(g.uni() * 4.0); }
+  int sense() { return g.uni() < 0.5 ? -1 : 1; }
+  M3 haar() { return g.haar(); }
+  double expo(double mean) { return -log(g.uni()) * mean; }
+  double gamma() { return -log(g.uni()); }
+  double uniform() { return g.uni(); }
+  int set_index() { return (int)(g.uni() * (double)ECMC_SET_SIZE); }
+  const M3& set_elem(int i) const { return (*set)[i]; }
+  void call_start() {}
+  void loop_start() {}
+  void on_lift() {}
+};
+
 // sample_persistant (ecmc_mpi_cb.cpp:496-637) for one chain: events until the chain has
 // travelled theta_sample; the state persists across calls.  The set of near-identity
 // elements is the call's shared set (the reference regenerates its per-rank set at every
 // call and every 10000 lifts).
-static void ecmc_chain(const EcmcBlock& blk, const EcmcParams& p, const std::vector<M3>& set, uint32_t chain,
-                       uint64_t seed, EcmcChain& st) {
+template <class D>
+static void ecmc_chain(const EcmcBlock& blk, const EcmcParams& p, D& g, EcmcChain& st) {
   Lat& f = *blk.f;
-  const int l = p.l_core;
-  EcmcStream g{chain, (uint32_t)seed, (uint32_t)(seed >> 32), &st.draws};
-  // random_site (ecmc_mpi_cb.cpp:359-367): local coordinates 1 .. l-2 (padded 2 .. L-1)
-  auto rand_site = [&](int lc[4]) {
-    for (int d = 0; d < 4; ++d) lc[d] = 1 + (int)(g.uni() * (double)(l - 2));
-  };
   M3 R;
   if (!st.initialized) {
-    rand_site(st.site);
-    st.mu = (int)(g.uni() * 4.0);
-    st.epsilon = g.uni() < 0.5 ? -1 : 1;
+    g.site(st.site);
+    st.mu = g.dir();
+    st.epsilon = g.sense();
     R = g.haar();
-    st.theta_refresh_site = p.poisson ? -log(g.uni()) * p.theta_refresh_site : p.theta_refresh_site;
-    st.theta_refresh_R = p.poisson ? -log(g.uni()) * p.theta_refresh_R : p.theta_refresh_R;
+    st.theta_refresh_site = p.poisson ? g.expo(p.theta_refresh_site) : p.theta_refresh_site;
+    st.theta_refresh_R = p.poisson ? g.expo(p.theta_refresh_R) : p.theta_refresh_R;
     st.travelled_site = st.travelled_R = 0.0;
     st.events = st.lifts = 0;
     st.initialized = 1;
   } else {
     memcpy(R.a, st.R, sizeof R.a);
   }
-  const double theta_sample = p.poisson ? -log(g.uni()) * p.theta_sample : p.theta_sample;
+  const double theta_sample = p.poisson ? g.expo(p.theta_sample) : p.theta_sample;
+  g.call_start();
   double trav_sample = 0.0;
   int lc[4] = {st.site[0], st.site[1], st.site[2], st.site[3]};
   int mu = st.mu, eps = st.epsilon;
@@ -770,6 +789,7 @@ static void ecmc_chain(const EcmcBlock& blk, const EcmcParams& p, const std::vec
       st.status |= 2;
       break;
     }
+    g.loop_start();
     const size_t x = blk.site(lc);
     const M3 U = f.get(x, mu);
     const M3 T = mul(adj(R), U);
@@ -784,11 +804,11 @@ static void ecmc_chain(const EcmcBlock& blk, const EcmcParams& p, const std::vec
       shifted(lc, mu, 1, nu, -1, d);  // x+mu-nu
       shifted(lc, nu, -1, -1, 0, e);  // x-nu
       M3 S = mul(blk.get(a, nu), adj(mul(f.get(x, nu), blk.get(c, mu))));
-      double rej = reject_angle(T, S, R, p.beta, -log(g.uni()), eps);
+      double rej = reject_angle(T, S, R, p.beta, g.gamma(), eps);
       if (k == 0 || rej < best) best = rej, j = k;
       ++k;
       S = mul(adj(mul(blk.get(e, mu), blk.get(d, nu))), blk.get(e, nu));
-      rej = reject_angle(T, S, R, p.beta, -log(g.uni()), eps);
+      rej = reject_angle(T, S, R, p.beta, g.gamma(), eps);
       if (rej < best) best = rej, j = k;
       ++k;
     }
@@ -821,16 +841,16 @@ static void ecmc_chain(const EcmcBlock& blk, const EcmcParams& p, const std::vec
       trav_sample += d_site;
       st.travelled_R += d_site;
       st.travelled_site = 0.0;
-      if (p.poisson) st.theta_refresh_site = -log(g.uni()) * p.theta_refresh_site;
-      rand_site(lc);
-      mu = (int)(g.uni() * 4.0);
-      eps = g.uni() < 0.5 ? -1 : 1;
+      if (p.poisson) st.theta_refresh_site = g.expo(p.theta_refresh_site);
+      g.site(lc);
+      mu = g.dir();
+      eps = g.sense();
     } else if (step == d_R) {
       update(d_R);
       trav_sample += d_R;
       st.travelled_site += d_R;
       st.travelled_R = 0.0;
-      if (p.poisson) st.theta_refresh_R = -log(g.uni()) * p.theta_refresh_R;
+      if (p.poisson) st.theta_refresh_R = g.expo(p.theta_refresh_R);
       R = g.haar();
     } else {
       update(best);
@@ -884,17 +904,17 @@ static void ecmc_chain(const EcmcBlock& blk, const EcmcParams& p, const std::vec
       double pr[4];
       for (int i = 0; i < 4; ++i) pr[i] = ab[i] / sum;
       // selectVariable (ecmc_mpi_cb.cpp:252-260)
-      const double r = g.uni();
+      const double r = g.uniform();
       const int idx = r < pr[0] ? 0 : (r < pr[0] + pr[1] ? 1 : (r < pr[0] + pr[1] + pr[2] ? 2 : 3));
-      const int iset = (int)(g.uni() * (double)ECMC_SET_SIZE);
-      const M3 Rn = mul(set[iset], R);
+      const int iset = g.set_index();
+      const M3 Rn = mul(g.set_elem(iset), R);
       const double ds_old = sg[idx] * ab[idx];
       const double ds_new = compute_ds(P[idx], Rn);
       int new_eps = -sg[idx];
       if (fabs(ds_old) < fabs(ds_new)) {
         R = Rn;
         new_eps = -dsign(ds_new);
-      } else if (g.uni() < fabs(ds_new) / fabs(ds_old)) {
+      } else if (g.uniform() < fabs(ds_new) / fabs(ds_old)) {
         R = Rn;
         new_eps = -dsign(ds_new);
       }
@@ -902,6 +922,7 @@ static void ecmc_chain(const EcmcBlock& blk, const EcmcParams& p, const std::vec
       for (int d = 0; d < 4; ++d) same = same && (lk[idx][d] == lc[d]);
       st.revs += same ? 1 : 0;
       st.lifts++;
+      g.on_lift();
       for (int d = 0; d < 4; ++d) lc[d] = lk[idx][d];
       mu = ld[idx];
       eps = new_eps;
@@ -912,6 +933,84 @@ static void ecmc_chain(const EcmcBlock& blk, const EcmcParams& p, const std::vec
   st.epsilon = eps;
   memcpy(st.R, R.a, sizeof R.a);
 }
+
+
+// The reference's own draws (one MPI rank, std::mt19937_64 rng(seed + rank)): the static
+// distributions of sample_persistant, random_site, lift_improved_fast and
+// compute_reject_angles_fast (ecmc_mpi_cb.cpp:197-567), random_su3 by Householder QR
+// (utils.cpp:13-30), and the rank's set of 10001 elements regenerated at the start of every
+// call and whenever set_counter % 10000 == 0 at the top of the event loop (:560-566).
+struct RefDraws {
+  std::mt19937_64* rng;
+  int l;
+  double eps_set;
+  std::vector<M3>* set;
+  uint64_t* set_counter;
+  std::uniform_int_distribution<int> coord, rdir, reps;
+  std::uniform_real_distribution<double> unif01;
+  RefDraws(std::mt19937_64* r, int l_, double e, std::vector<M3>* s, uint64_t* sc)
+      : rng(r), l(l_), eps_set(e), set(s), set_counter(sc), coord(2, l_ - 1), rdir(0, 3), reps(0, 1), unif01(0.0, 1.0) {}
+  void site(int lc[4]) {
+    for (int d = 0; d < 4; ++d) lc[d] = coord(*rng) - 1;  // padded x, y, z, t -> local
+  }
+  int dir() { return rdir(*rng); }
+  int sense() { return 2 * reps(*rng) - 1; }
+  M3 haar() { return random_su3_ref(*rng); }
+  double expo(double mean) { return std::exponential_distribution<double>(1.0 / mean)(*rng); }
+  double gamma() { return -std::log(unif01(*rng)); }
+  double uniform() { return unif01(*rng); }
+  int set_index() { return (int)std::uniform_int_distribution<size_t>(0, set->size() - 1)(*rng); }
+  const M3& set_elem(int i) const { return (*set)[i]; }
+  // ecmc_set with random_SU3_epsilon (utils.cpp:66-127): 9 uniforms in (-1/2, 1/2) per pair
+  void regenerate() {
+    std::uniform_real_distribution<double> u(-0.5, 0.5);
+    set->assign(ECMC_SET_SIZE, ident());
+    for (int pidx = 0; pidx < (ECMC_SET_SIZE - 1) / 2; ++pidx) {
+      double r[9];
+      for (int d = 0; d < 9; ++d) r[d] = u(*rng);
+      (*set)[2 * pidx + 1] = su3_near_identity(eps_set, r);
+      (*set)[2 * pidx + 2] = adj((*set)[2 * pidx + 1]);
+    }
+  }
+  void call_start() { regenerate(); }
+  void loop_start() {
+    if (*set_counter % 10000 == 0) {
+      regenerate();
+      *set_counter = 0;
+    }
+  }
+  void on_lift() { ++*set_counter; }
+};
+
+// generate_ecmc_cb on one rank (n_core_dims = 1, src/bin/gauge_ecmc_ncb.cpp:20-269): the
+// lattice is one L^4 block with frozen faces; each shift is random_shift (field moved) then
+// sample_persistant.
+struct RefEcmcRun {
+  int dims[4];
+  std::vector<C> links, tmp;
+  std::mt19937_64 rng;
+  EcmcParams p;
+  EcmcChain st;
+  std::vector<M3> set;
+  uint64_t set_counter = 0;
+  Lat lat() {
+    Lat l;
+    for (int d = 0; d < 4; ++d) l.L[d] = dims[d];
+    l.V = (size_t)dims[0] * dims[1] * dims[2] * dims[3];
+    l.u = links.data();
+    return l;
+  }
+  void shift_and_sample() {
+    Lat f = lat();
+    random_shift(f, rng, tmp);
+    RefDraws g(&rng, p.l_core, p.epsilon_set, &set, &set_counter);
+    EcmcBlock blk;
+    blk.f = &f;
+    blk.l = p.l_core;
+    for (int d = 0; d < 4; ++d) blk.b[d] = blk.cum[d] = 0;
+    ecmc_chain(blk, p, g, st);
+  }
+};
 
 }  // namespace orc
 
@@ -1151,8 +1250,60 @@ int orc_ecmc_sample(double* aos, const int dims[4], const double dp[5], const in
       for (int bz = 0; bz < nb[2]; ++bz)
         for (int bt = 0; bt < nb[3]; ++bt, ++id) {
           blk.b[0] = bx, blk.b[1] = by, blk.b[2] = bz, blk.b[3] = bt;
-          ecmc_chain(blk, p, set, id, seed, st[id]);
+          LibDraws g{EcmcStream{id, (uint32_t)seed, (uint32_t)(seed >> 32), &st[id].draws}, &set, l};
+          ecmc_chain(blk, p, g, st[id]);
         }
+  return 0;
+}
+
+// generate_ecmc_cb on one rank with the reference's generator: create (cold or hot start
+// with random_su3 per link), then n_shift x (random_shift + sample_persistant) with the
+// plaquette after each shift; counters out[0..2] = events, lifts, same-site lifts so far.
+void* orc_ecmc_ref_create(int L, int seed, int cold_start, const double dp[5], const int ip[2]) {
+  RefEcmcRun* r = new RefEcmcRun();
+  for (int d = 0; d < 4; ++d) r->dims[d] = L;
+  const size_t V = (size_t)L * L * L * L;
+  r->links.assign(V * 36, C(0.0, 0.0));
+  r->rng.seed((uint64_t)(int64_t)seed + 0);  // rp.seed + topo.rank
+  r->p = EcmcParams{dp[0], dp[1], dp[2], dp[3], dp[4], ip[0], L};
+  (void)ip[1];
+  memset(&r->st, 0, sizeof r->st);
+  Lat f = r->lat();
+  for (size_t s = 0; s < V; ++s)
+    for (int mu = 0; mu < 4; ++mu) f.set(s, mu, ident());
+  if (!cold_start)
+    for (size_t s = 0; s < V; ++s)
+      for (int mu = 0; mu < 4; ++mu) f.set(s, mu, random_su3_ref(r->rng));
+  return r;
+}
+
+void orc_ecmc_ref_destroy(void* h) { delete static_cast<RefEcmcRun*>(h); }
+
+int orc_ecmc_ref_run(void* h, int n_shift, double* plaq, uint64_t* counters) {
+  RefEcmcRun* r = static_cast<RefEcmcRun*>(h);
+  for (int i = 0; i < n_shift; ++i) {
+    r->shift_and_sample();
+    if (plaq) {
+      Lat f = r->lat();
+      plaq[i] = plaquette_sum(f) / (6.0 * (double)f.V);
+    }
+  }
+  if (counters) {
+    counters[0] = r->st.events;
+    counters[1] = r->st.lifts;
+    counters[2] = r->st.revs;
+  }
+  return 0;
+}
+
+int orc_ecmc_ref_get_links(void* h, double* aos) {
+  RefEcmcRun* r = static_cast<RefEcmcRun*>(h);
+  memcpy(aos, r->links.data(), r->links.size() * sizeof(C));
+  return 0;
+}
+int orc_ecmc_ref_set_links(void* h, const double* aos) {
+  RefEcmcRun* r = static_cast<RefEcmcRun*>(h);
+  memcpy(r->links.data(), aos, r->links.size() * sizeof(C));
   return 0;
 }
 

@@ -202,3 +202,35 @@ def test_equilibrium_matches_heatbath(ctx):
     assert abs(np.mean(ep) - np.mean(hp)) < 4 * np.hypot(err(ep), err(hp)), (np.mean(ep), np.mean(hp))
     ch.close()
     f.close()
+
+
+def test_gpu_chains_sample_as_the_reference_generator(ctx):
+    """The GPU chain (Philox, the library's shared set) and the restatement with the
+    reference's own generator (std::mt19937_64) on the same setup, one rank's 6^4 block with
+    frozen faces at beta = 2, from the same heatbath-equilibrated start, keep the same mean
+    plaquette."""
+    dims, beta = (6, 6, 6, 6), 2.0
+    p = dict(BASE, beta=beta, theta_sample=40.0, l_core=6)
+    start, _ = orc.heatbath_cb(orc.cold(dims), dims, beta, 60, 1, 31, 0)  # equilibrated start
+    ref = orc.EcmcRefRun(6, 4321, True, p)
+    ref.set_links(start)
+    rplaq, _ = ref.run(600)
+    f = qcb.GaugeField(ctx, dims)
+    f.set_links(start)
+    ch = qcb.EventChains(f, p, 17)
+    rng = np.random.default_rng(3)
+    cum = np.zeros(4, int)
+    gp = []
+    for call in range(600):
+        cum = (cum + rng.integers(0, 6, 4)) % 6
+        ch.sample(cum)
+        gp.append(qcb.observables.mean_plaquette_global(f))
+    a, b = np.asarray(gp[100:]), rplaq[100:]
+
+    def err(x, nb=10):
+        n = len(x) // nb
+        return x[:n * nb].reshape(nb, n).mean(1).std() / np.sqrt(nb)
+
+    assert abs(a.mean() - b.mean()) < 4 * np.hypot(err(a), err(b)) + 1e-4, (a.mean(), b.mean())
+    ch.close()
+    f.close()

@@ -162,3 +162,33 @@ def test_equilibrium_matches_heatbath_strong_coupling():
 
     diff = abs(np.mean(ep) - np.mean(hp))
     assert diff < 4 * np.hypot(err(ep), err(hp)) + 1e-4, (np.mean(ep), np.mean(hp), err(ep), err(hp))
+
+
+def _binned_err(x, nb=10):
+    x = np.asarray(x)
+    n = len(x) // nb
+    return x[:n * nb].reshape(nb, n).mean(1).std() / np.sqrt(nb)
+
+
+def test_reference_generator_chain_matches_heatbath():
+    """The restatement with the reference's own generator (std::mt19937_64, std::
+    distributions, Householder random_su3, per-rank set regenerated per call and every 10000
+    lifts) on one rank: 6^4 as one block with frozen faces, moved by random_shift each call.
+    From a heatbath-equilibrated start at beta = 2 it keeps the heatbath's mean plaquette;
+    links stay unitary."""
+    dims, beta = (6, 6, 6, 6), 2.0
+    uh = orc.cold(dims)
+    hp = []
+    for s in range(160):
+        uh, _ = orc.heatbath_cb(uh, dims, beta, 1, 1, 29, s)
+        if s >= 40:
+            hp.append(orc.plaquette(uh, dims))
+    run = orc.EcmcRefRun(6, 4321, True, dict(PARAMS, beta=beta, theta_sample=40.0))
+    run.set_links(uh)  # from the heatbath's equilibrium
+    plaq, (events, lifts, revs) = run.run(500)
+    ep = plaq[50:]
+    assert events >= lifts > revs > 0
+    assert abs(np.mean(ep) - np.mean(hp)) < 4 * np.hypot(_binned_err(ep), _binned_err(hp)) + 1e-4, \
+        (np.mean(ep), np.mean(hp))
+    U = run.links().reshape(-1, 3, 3)
+    assert np.abs(np.einsum("nij,nkj->nik", U, U.conj()) - np.eye(3)).max() < 1e-11
