@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(64) k_ecmc_sample(EcmcLaunch a) {
   int lc[4], mu, eps;
   double th_site, th_R, tr_site, tr_R;
   uint64_t events, lifts, revs = rec.revs;
-  int status = rec.status;
+  int status = 0;  // the record keeps the bits of the latest call
   M R;
   if (!rec.initialized) {
     // random_site (ecmc_mpi_cb.cpp:359-367): local coordinates 1 .. l-2 (padded 2 .. L-1)

@@ -357,7 +357,7 @@ typedef struct qcb_ecmc_chain {
   int32_t site[4];            /* block-local x, y, z, t of the active link, in [0, l_core) */
   int32_t mu, epsilon;        /* direction of the active link, sense of rotation (+1 / -1) */
   int32_t initialized;        /* 0: drawn at the next call (site, mu, epsilon, R, budgets) */
-  int32_t status;             /* bit 0: non-finite event angle; bit 1: 2^26 events in one call */
+  int32_t status;             /* latest call: bit 0 non-finite event angle; bit 1 2^26 events */
   int32_t pad[4];
 } qcb_ecmc_chain;
 int qcb_ecmc_create(qcb_lattice* lat, const qcb_ecmc_params* params, uint64_t seed, qcb_ecmc** out);
@@ -367,8 +367,9 @@ int qcb_ecmc_num_chains(const qcb_ecmc* e, int* n);
 int qcb_ecmc_sample(qcb_ecmc* e, const int shift[4]);
 /* Waits, then sums the chains' events, lifts and same-site lifts into out[0..2]; with reset,
  * zeroes the three counters afterwards (the reference resets them after each plaquette
- * measurement).  A chain that stopped on a non-finite angle or the event cap returns
- * QCB_ERR_STATE (its bits are cleared). */
+ * measurement).  If a chain stopped early (non-finite event angle, or 2^26 events in one
+ * call) since the previous check, returns QCB_ERR_STATE once; the chain records keep the
+ * status bits of their latest call. */
 int qcb_ecmc_counters(qcb_ecmc* e, uint64_t out[3], int reset);
 /* Copies the chain records (qcb_ecmc_num_chains of them) and the number of sample calls
  * made so far (the key of the next call's set) to / from host memory; synchronous. */

@@ -765,6 +765,7 @@ struct LibDraws {
 template <class D>
 static void ecmc_chain(const EcmcBlock& blk, const EcmcParams& p, D& g, EcmcChain& st) {
   Lat& f = *blk.f;
+  st.status = 0;  // the record keeps the bits of the latest call
   M3 R;
   if (!st.initialized) {
     g.site(st.site);

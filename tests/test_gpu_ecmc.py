@@ -234,3 +234,29 @@ def test_gpu_chains_sample_as_the_reference_generator(ctx):
     assert abs(a.mean() - b.mean()) < 4 * np.hypot(err(a), err(b)) + 1e-4, (a.mean(), b.mean())
     ch.close()
     f.close()
+
+
+def test_non_finite_angle_stops_the_chain_and_is_reported(ctx):
+    """Links with NaN give a non-finite event angle: every chain stops at its first event,
+    records status bit 0, and qcb_ecmc_counters reports QCB_ERR_STATE once; with valid links
+    the same object samples again."""
+    dims = (8, 8, 8, 8)
+    f = qcb.GaugeField(ctx, dims)
+    f.set_links(np.full(orc.shape(dims), np.nan + 0j))
+    ch = qcb.EventChains(f, BASE, 3)
+    ch.sample((0, 0, 0, 0))
+    with pytest.raises(qcb.QcbError) as e:
+        ch.counters(reset=True)
+    assert e.value.code == 7 and "non-finite" in str(e.value)
+    rec, _ = ch.chains()
+    assert (rec["status"] & 1).all() and (rec["events"] == 0).all()
+    u = orc.hot_philox(dims, 4)
+    f.set_links(u)
+    ch.set_chains(rec, 1)
+    ch.sample((1, 0, 0, 0))
+    assert ch.counters()[0] > 0
+    assert (ch.chains()[0]["status"] == 0).all()
+    ref_u, _ = orc.ecmc_sample(u, dims, BASE, 3, 1, (1, 0, 0, 0), rec)
+    assert np.abs(f.get_links() - ref_u).max() < 1e-9
+    ch.close()
+    f.close()

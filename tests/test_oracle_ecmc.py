@@ -192,3 +192,10 @@ def test_reference_generator_chain_matches_heatbath():
         (np.mean(ep), np.mean(hp))
     U = run.links().reshape(-1, 3, 3)
     assert np.abs(np.einsum("nij,nkj->nik", U, U.conj()) - np.eye(3)).max() < 1e-11
+
+
+def test_non_finite_angle_stops_the_chain():
+    dims = (8, 8, 8, 8)
+    u = np.full(orc.shape(dims), np.nan + 0j)
+    _, ch = orc.ecmc_sample(u, dims, PARAMS, 3, 0, (0, 0, 0, 0), orc.ecmc_chains(dims, 4))
+    assert (ch["status"] & 1).all() and (ch["events"] == 0).all() and (ch["initialized"] == 1).all()
