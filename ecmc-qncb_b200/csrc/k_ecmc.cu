@@ -12,8 +12,10 @@
 //
 // Random numbers: chain c's k-th uniform is Philox4x32-10 with counter (k_lo, k_hi, c,
 // ECMC_CHAIN) and key seed; the call's set of near-identity elements uses counters
-// (j, call_lo, call_hi, ECMC_SET).  The arithmetic follows the reference's order of
-// operations, so the CPU oracle (same counters) reproduces every event.
+// (j, call_lo, call_hi, ECMC_SET).  The arithmetic is the reference's up to the order of
+// the floating-point operations (products streamed by rows, dS as a trace against
+// R diag(1, -1, 0) R^dagger), so the CPU oracle, drawing from the same counters, takes the
+// same events with links equal to rounding.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
