@@ -440,6 +440,19 @@ def _ecmc_cpu_worker(args):
     return events - events0, time.perf_counter() - t
 
 
+def ecmc_cpu_reference(budget_s: float = 8.0) -> dict:
+    """The reference's event-chain algorithm with its own generator on the host cores, one
+    process per core as one rank each (see _ecmc_cpu_worker)."""
+    cores = min(64, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1))
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_ecmc_cpu_worker, [(500 + r, budget_s) for r in range(cores)])
+    return {"value": sum(r[0] for r in res) / max(r[1] for r in res), "unit": "events/s", "cores": cores,
+            "kind": "port",
+            "sample": f"{cores} processes, each one rank of the reference (one chain on a {ECMC_LCORE}^4 block, the "
+                      f"reference's std::mt19937_64 generator and per-call set), theta_sample {ECMC_THETA:g} calls "
+                      f"for {budget_s:g} s"}
+
+
 def ecmc_section(ctx, steps=5, warmup=3, cpu_budget_s=8.0, cpu=True):
     """Event-chain Monte Carlo: a 64^4 FP64 lattice as 16^4 blocks of 4^4 (65536 chains, one
     per block, as 65536 ranks of the reference would run), beta = 6.0, from a Haar hot start
@@ -507,14 +520,7 @@ def ecmc_section(ctx, steps=5, warmup=3, cpu_budget_s=8.0, cpu=True):
     ch.close()
     f.close()
     if cpu:
-        cores = min(64, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1))
-        with mp.get_context("spawn").Pool(cores) as pool:
-            res = pool.map(_ecmc_cpu_worker, [(500 + r, cpu_budget_s) for r in range(cores)])
-        out["cpu_baseline"] = {"value": sum(r[0] for r in res) / max(r[1] for r in res), "unit": "events/s",
-                               "cores": cores, "kind": "port",
-                               "sample": f"{cores} processes, each one rank of the reference (one chain on a "
-                                         f"{ECMC_LCORE}^4 block, the reference's std::mt19937_64 generator and "
-                                         f"per-call set), theta_sample {ECMC_THETA:g} calls for {cpu_budget_s:g} s"}
+        out["cpu_baseline"] = ecmc_cpu_reference(cpu_budget_s)
     return out
 
 
@@ -837,6 +843,7 @@ def main():
                "config": {"workload": "precision 32^4 (reference schedule, 16^4 blocks per core), beta=6.0, "
                                       "hot start; sweep and RK3 flow rates", "lattice": [L, L, L, L]},
                "flow": {"value": statistics.mean(r["flow_value"] for r in timed), "unit": "site-steps/s"},
+               "ecmc": ecmc_cpu_reference(),
                "cpu_baseline": cb,
                "e2e": {"value": v, "unit": "link-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(out))
