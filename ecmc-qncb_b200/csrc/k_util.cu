@@ -191,16 +191,13 @@ __device__ __forceinline__ double bswap_d(double v) {
   return __longlong_as_double(((unsigned long long)lo << 32) | hi);
 }
 
-// One thread per (site of the chunk, mu).  aos points at the chunk's first site, site0.
-template <typename S, int NR>
-__global__ void k_aos_to_soa(Geom g, Links<S, NR> f, const double* __restrict__ aos, uint32_t site0,
-                             uint32_t nsites, int bswap) {
-  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (uint64_t)nsites * 4) return;
-  const uint32_t sl = (uint32_t)(t >> 2);
-  const int mu = (int)(t & 3);
-  const uint32_t s = site0 + sl;
-  // parity of s
+// One thread per (site of the chunk, mu), blocks of AOS_BLOCK threads.  The AoS side of a
+// block is one contiguous run of AOS_BLOCK links (144 bytes each), moved between global and
+// shared memory in 16-byte chunks by consecutive threads (coalesced); each thread then
+// converts its own link.  aos points at the chunk's first site, site0 (16-byte aligned).
+constexpr int AOS_BLOCK = 128;
+
+__device__ __forceinline__ int site_parity(const Geom& g, uint32_t s) {
   uint32_t r = s;
   const int x = (int)(r % (uint32_t)g.L[0]);
   r /= (uint32_t)g.L[0];
@@ -208,63 +205,76 @@ __global__ void k_aos_to_soa(Geom g, Links<S, NR> f, const double* __restrict__ 
   r /= (uint32_t)g.L[1];
   const int z = (int)(r % (uint32_t)g.L[2]);
   const int tt = (int)(r / (uint32_t)g.L[2]);
-  const int par = (x + y + z + tt) & 1;
-  const double* src = aos + ((size_t)sl * 4 + mu) * 18;
+  return (x + y + z + tt) & 1;
+}
+
+template <typename S, int NR>
+__global__ void __launch_bounds__(AOS_BLOCK) k_aos_to_soa(Geom g, Links<S, NR> f, const double* __restrict__ aos,
+                                                          uint32_t site0, uint32_t nsites, int bswap) {
+  __shared__ double2 sm[AOS_BLOCK * 9];
+  const uint64_t t0 = (uint64_t)blockIdx.x * AOS_BLOCK, nlinks = (uint64_t)nsites * 4;
+  const uint32_t nl = (uint32_t)min((uint64_t)AOS_BLOCK, nlinks - t0);
+  const double2* src = reinterpret_cast<const double2*>(aos) + t0 * 9;
+  for (uint32_t c = threadIdx.x; c < nl * 9; c += AOS_BLOCK) sm[c] = src[c];
+  __syncthreads();
+  if (threadIdx.x >= nl) return;
+  const uint64_t t = t0 + threadIdx.x;
+  const uint32_t sl = (uint32_t)(t >> 2);
+  const int mu = (int)(t & 3);
+  const uint32_t s = site0 + sl;
   m3<double> u;
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
-    double re = src[2 * k], im = src[2 * k + 1];
+    const double2 v = sm[threadIdx.x * 9 + k];
+    double re = v.x, im = v.y;
     if (bswap) {
       re = bswap_d(re);
       im = bswap_d(im);
     }
     u.e[k / 3][k % 3] = mk<double>(re, im);
   }
-  f.template store<double>(mu, par, s >> 1, u);
+  f.template store<double>(mu, site_parity(g, s), s >> 1, u);
 }
 
 template <typename S, int NR>
-__global__ void k_soa_to_aos(Geom g, Links<S, NR> f, double* __restrict__ aos, uint32_t site0, uint32_t nsites,
-                             int bswap) {
-  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (uint64_t)nsites * 4) return;
-  const uint32_t sl = (uint32_t)(t >> 2);
-  const int mu = (int)(t & 3);
-  const uint32_t s = site0 + sl;
-  uint32_t r = s;
-  const int x = (int)(r % (uint32_t)g.L[0]);
-  r /= (uint32_t)g.L[0];
-  const int y = (int)(r % (uint32_t)g.L[1]);
-  r /= (uint32_t)g.L[1];
-  const int z = (int)(r % (uint32_t)g.L[2]);
-  const int tt = (int)(r / (uint32_t)g.L[2]);
-  const int par = (x + y + z + tt) & 1;
-  const m3<double> u = f.template load<double>(mu, par, s >> 1);
-  double* dst = aos + ((size_t)sl * 4 + mu) * 18;
+__global__ void __launch_bounds__(AOS_BLOCK) k_soa_to_aos(Geom g, Links<S, NR> f, double* __restrict__ aos,
+                                                          uint32_t site0, uint32_t nsites, int bswap) {
+  __shared__ double2 sm[AOS_BLOCK * 9];
+  const uint64_t t0 = (uint64_t)blockIdx.x * AOS_BLOCK, nlinks = (uint64_t)nsites * 4;
+  const uint32_t nl = (uint32_t)min((uint64_t)AOS_BLOCK, nlinks - t0);
+  if (threadIdx.x < nl) {
+    const uint64_t t = t0 + threadIdx.x;
+    const uint32_t sl = (uint32_t)(t >> 2);
+    const int mu = (int)(t & 3);
+    const uint32_t s = site0 + sl;
+    const m3<double> u = f.template load<double>(mu, site_parity(g, s), s >> 1);
 #pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    double re = u.e[k / 3][k % 3].re, im = u.e[k / 3][k % 3].im;
-    if (bswap) {
-      re = bswap_d(re);
-      im = bswap_d(im);
+    for (int k = 0; k < 9; ++k) {
+      double re = u.e[k / 3][k % 3].re, im = u.e[k / 3][k % 3].im;
+      if (bswap) {
+        re = bswap_d(re);
+        im = bswap_d(im);
+      }
+      sm[threadIdx.x * 9 + k] = make_double2(re, im);
     }
-    dst[2 * k] = re;
-    dst[2 * k + 1] = im;
   }
+  __syncthreads();
+  double2* dst = reinterpret_cast<double2*>(aos) + t0 * 9;
+  for (uint32_t c = threadIdx.x; c < nl * 9; c += AOS_BLOCK) dst[c] = sm[c];
 }
 
 template <typename S, int NR>
 static cudaError_t a2s_impl(const LatDev& L, const double* aos, uint32_t site0, uint32_t nsites, int bswap,
-                            cudaStream_t s, int block) {
-  k_aos_to_soa<S, NR><<<grid_for((uint64_t)nsites * 4, block), block, 0, s>>>(L.g, links_of<S, NR>(L), aos, site0,
-                                                                               nsites, bswap);
+                            cudaStream_t s, int) {
+  k_aos_to_soa<S, NR><<<grid_for((uint64_t)nsites * 4, AOS_BLOCK), AOS_BLOCK, 0, s>>>(L.g, links_of<S, NR>(L), aos,
+                                                                                     site0, nsites, bswap);
   return cudaGetLastError();
 }
 template <typename S, int NR>
 static cudaError_t s2a_impl(const LatDev& L, double* aos, uint32_t site0, uint32_t nsites, int bswap,
-                            cudaStream_t s, int block) {
-  k_soa_to_aos<S, NR><<<grid_for((uint64_t)nsites * 4, block), block, 0, s>>>(L.g, links_of<S, NR>(L), aos, site0,
-                                                                               nsites, bswap);
+                            cudaStream_t s, int) {
+  k_soa_to_aos<S, NR><<<grid_for((uint64_t)nsites * 4, AOS_BLOCK), AOS_BLOCK, 0, s>>>(L.g, links_of<S, NR>(L), aos,
+                                                                                     site0, nsites, bswap);
   return cudaGetLastError();
 }
 cudaError_t launch_aos_to_soa(const LatDev& L, const double* aos, uint32_t site0, uint32_t nsites, int bswap,
