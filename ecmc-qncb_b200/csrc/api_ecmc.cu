@@ -124,8 +124,10 @@ int qcb_ecmc_num_chains(const qcb_ecmc* e, int* n) {
   return QCB_OK;
 }
 
-int qcb_ecmc_sample(qcb_ecmc* e, const int shift[4]) {
-  if (!e || !shift) return efail(QCB_ERR_INVALID, "null argument");
+int qcb_ecmc_sample_n(qcb_ecmc* e, const int* shifts, int n) {
+  if (!e || (!shifts && n > 0)) return efail(QCB_ERR_INVALID, "null argument");
+  if (n < 0) return efail(QCB_ERR_INVALID, "negative call count");
+  if (n == 0) return QCB_OK;
   qcb_lattice* L = e->lat;
   qcb_ctx* c = e->ctx;
   EcmcLaunch a;
@@ -136,7 +138,6 @@ int qcb_ecmc_sample(qcb_ecmc* e, const int shift[4]) {
   for (int d = 0; d < 4; ++d) {
     a.L[d] = L->dev.g.L[d];
     a.nb[d] = e->nb[d];
-    a.cum[d] = ((shift[d] % a.L[d]) + a.L[d]) % a.L[d];
   }
   a.l = e->p.l_core;
   a.beta = e->p.beta;
@@ -151,13 +152,23 @@ int qcb_ecmc_sample(qcb_ecmc* e, const int shift[4]) {
   ECU(cudaSetDevice(c->device), "cudaSetDevice");
   ECU(launch_soa_to_aos(L->dev, reinterpret_cast<double*>(e->d_links), 0, L->dev.g.V, 0, c->stream, 0),
       "links to FP64 array-of-structures");
-  ECU(launch_ecmc_set(e->d_set, e->p.epsilon_set, e->seed, e->calls, c->stream), "ECMC set");
-  ECU(launch_ecmc_sample(a, c->stream, 0), "ECMC sample");
+  c->launches++;
+  for (int k = 0; k < n; ++k) {
+    for (int d = 0; d < 4; ++d) a.cum[d] = ((shifts[4 * k + d] % a.L[d]) + a.L[d]) % a.L[d];
+    ECU(launch_ecmc_set(e->d_set, e->p.epsilon_set, e->seed, e->calls, c->stream), "ECMC set");
+    ECU(launch_ecmc_sample(a, c->stream, 0), "ECMC sample");
+    c->launches += 2;
+    e->calls++;
+  }
   ECU(launch_aos_to_soa(L->dev, reinterpret_cast<const double*>(e->d_links), 0, L->dev.g.V, 0, c->stream, 0),
       "links from FP64 array-of-structures");
-  c->launches += 4;
-  e->calls++;
+  c->launches++;
   return QCB_OK;
+}
+
+int qcb_ecmc_sample(qcb_ecmc* e, const int shift[4]) {
+  if (!e || !shift) return efail(QCB_ERR_INVALID, "null argument");
+  return qcb_ecmc_sample_n(e, shift, 1);
 }
 
 int qcb_ecmc_counters(qcb_ecmc* e, uint64_t out[3], int reset) {

@@ -125,6 +125,7 @@ struct Run {
   int n_chains = 0;
   uint64_t key = 0;
   int cum[4] = {0, 0, 0, 0};  // cumulative shift not yet applied to the stored links
+  std::vector<int> pending;   // cumulative shifts of sample calls not yet launched
   std::mt19937_64 shift_rng;
   std::vector<size_t> event_nb, lift_nb, rev_nb;
   std::vector<double> lambda;
@@ -137,17 +138,27 @@ struct Run {
     return rd.path() / (rd.name + "_seed") / (rd.name + "_seed" + std::to_string(r) + ".txt");
   }
 
-  // mpi::shift::random_shift + mpi::ecmccb::sample_persistant on every rank.
+  // mpi::shift::random_shift + mpi::ecmccb::sample_persistant on every rank.  The sample
+  // calls between two measurements are launched together (one pack and one unpack of the
+  // lattice): flush() runs them before anything reads the links or the chains.
   void shift_and_sample() {
     std::uniform_int_distribution<int> rand_l_shift(0, rp.L_core - 1);
     int s[4];
     for (int d = 0; d < 4; ++d) s[d] = rand_l_shift(shift_rng);
     std::cout << "Shift (" << s[0] << ", " << s[1] << ", " << s[2] << ", " << s[3] << ")\n";
     const int Lg = rp.L_core * rp.n_core_dims;
-    for (int d = 0; d < 4; ++d) cum[d] = (cum[d] + s[d]) % Lg;
-    CHECK(qcb_ecmc_sample(ecmc, cum), "ECMC sample");
+    for (int d = 0; d < 4; ++d) {
+      cum[d] = (cum[d] + s[d]) % Lg;
+      pending.push_back(cum[d]);
+    }
+  }
+  void flush() {
+    if (pending.empty()) return;
+    CHECK(qcb_ecmc_sample_n(ecmc, pending.data(), (int)(pending.size() / 4)), "ECMC sample");
+    pending.clear();
   }
   double plaquette() {
+    flush();
     double p = 0;
     CHECK(qcb_plaquette(lat, &p), "plaquette");
     return p;
@@ -155,6 +166,7 @@ struct Run {
   // Event counting after a plaquette sample (gauge_ecmc_ncb.cpp:176-210): lambda is the
   // angle travelled by all chains since the last sample over their lifts.
   void count_events() {
+    flush();
     uint64_t c[3];
     CHECK(qcb_ecmc_counters(ecmc, c, 1), "ECMC counters");
     const double total = (double)rp.N_shift_plaquette * rp.ecmc.theta_sample * (double)n_chains;
@@ -168,6 +180,7 @@ struct Run {
               << " (Reversibility : " << (double)avg_rev / (double)avg_lift * 100 << "%)\n";
   }
   std::vector<double> topo() {
+    flush();
     std::vector<double> tqe(3 * (size_t)rp.N_steps_gf);
     const double eps = 0.02;  // hard-coded in the reference driver (gauge_ecmc_ncb.cpp:62)
     CHECK(qcb_flow_measure(lat, eps, rp.N_steps_gf, rp.N_rk_steps, tqe.data()), "flow");
@@ -195,6 +208,7 @@ struct Run {
     lambda.clear();
   }
   void save_conf() {
+    flush();
     if (cum[0] | cum[1] | cum[2] | cum[3]) {
       // the blocks keep their place: after U'(x) = U(x - cum) they start at b * L_core
       CHECK(qcb_translate(lat, cum), "translate");
@@ -208,6 +222,7 @@ struct Run {
   // io::save_state (io.cpp:140-192) per chain, site as the index of the reference's padded
   // block ((t Lext + z) Lext + y) Lext + x with coordinates local + 1; plus the seed files.
   void save_state() {
+    flush();
     std::vector<qcb_ecmc_chain> ch(n_chains);
     uint64_t calls = 0;
     CHECK(qcb_ecmc_get_chains(ecmc, ch.data(), &calls), "ECMC chains");
@@ -318,14 +333,13 @@ void generate_ecmc_cb(Run& R, bool existing, int precision, int storage, int dev
       std::cout << "====== Plaquette ======\n";
       std::cout << "(Therm) Sample " << i / rp.N_shift_plaquette << ", <P> = " << p << "\n";
     }
-    uint64_t c[3];
-    CHECK(qcb_ecmc_counters(R.ecmc, c, 1), "ECMC counters");
   }
   std::cout << "\n\n===========================================\n";
   std::cout << "Sampling : " << rp.N_shift / rp.N_shift_plaquette << " <P> samples, " << rp.N_shift / rp.N_shift_topo
             << " Q samples\n";
   std::cout << "===========================================\n";
-  {
+  {  // the thermalisation's events are not counted (gauge_ecmc_ncb.cpp:122-130)
+    R.flush();
     uint64_t c[3];
     CHECK(qcb_ecmc_counters(R.ecmc, c, 1), "ECMC counters");
   }
@@ -368,6 +382,7 @@ void generate_ecmc_cb(Run& R, bool existing, int precision, int storage, int dev
   R.save_conf();
   R.save_state();
   std::cout << "==========================================\n";
+  R.flush();
   CHECK(qcb_ctx_sync(R.ctx), "sync");
   qcb_ecmc_destroy(R.ecmc);
   qcb_lattice_destroy(R.lat);

@@ -171,6 +171,7 @@ SIGNATURES = {
     "qcb_ecmc_destroy": (C.c_int, [_vp]),
     "qcb_ecmc_num_chains": (C.c_int, [_vp, _ip]),
     "qcb_ecmc_sample": (C.c_int, [_vp, _ip]),
+    "qcb_ecmc_sample_n": (C.c_int, [_vp, _ip, C.c_int]),
     "qcb_ecmc_counters": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int]),
     "qcb_ecmc_get_chains": (C.c_int, [_vp, _vp, C.POINTER(C.c_uint64)]),
     "qcb_ecmc_set_chains": (C.c_int, [_vp, _vp, C.c_uint64]),

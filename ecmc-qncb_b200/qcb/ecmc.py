@@ -58,6 +58,12 @@ class EventChains:
         """One sample call of every chain (asynchronous); shift = cumulative shift of the field."""
         check(lib().qcb_ecmc_sample(self.h, (C.c_int * 4)(*[int(s) for s in shift])))
 
+    def sample_n(self, shifts) -> None:
+        """Consecutive sample calls, one per row of cumulative shifts (n x 4), with one pack
+        and one unpack of the lattice; the same result as sample() per row."""
+        sh = np.ascontiguousarray(np.asarray(shifts, dtype=np.int32).reshape(-1, 4))
+        check(lib().qcb_ecmc_sample_n(self.h, sh.ctypes.data_as(C.POINTER(C.c_int)), int(sh.shape[0])))
+
     def counters(self, reset: bool = False):
         """(events, lifts, same-site lifts) summed over the chains."""
         out = (C.c_uint64 * 3)()

@@ -365,6 +365,10 @@ int qcb_ecmc_destroy(qcb_ecmc* e);
 int qcb_ecmc_num_chains(const qcb_ecmc* e, int* n);
 /* One sample call of every chain (asynchronous).  shift = cumulative shift of the field. */
 int qcb_ecmc_sample(qcb_ecmc* e, const int shift[4]);
+/* n sample calls in a row, call k with the cumulative shift shifts[4k .. 4k+3], with the
+ * lattice packed into the chains' FP64 copy once before and unpacked once after: the same
+ * result as n qcb_ecmc_sample calls, bit for bit (asynchronous). */
+int qcb_ecmc_sample_n(qcb_ecmc* e, const int* shifts, int n);
 /* Waits, then sums the chains' events, lifts and same-site lifts into out[0..2]; with reset,
  * zeroes the three counters afterwards (the reference resets them after each plaquette
  * measurement).  If a chain stopped early (non-finite event angle, or 2^26 events in one

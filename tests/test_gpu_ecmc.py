@@ -260,3 +260,26 @@ def test_non_finite_angle_stops_the_chain_and_is_reported(ctx):
     assert np.abs(f.get_links() - ref_u).max() < 1e-9
     ch.close()
     f.close()
+
+
+def test_sample_n_equals_single_calls(ctx):
+    """qcb_ecmc_sample_n (one pack and unpack for several calls) = the same calls one by one."""
+    dims = (8, 8, 8, 8)
+    u = orc.hot_philox(dims, 12)
+    shifts = np.array([[1, 0, 2, 3], [2, 3, 2, 0], [3, 1, 1, 1]])
+    fa = qcb.GaugeField(ctx, dims)
+    fa.set_links(u)
+    a = qcb.EventChains(fa, BASE, 41)
+    for s in shifts:
+        a.sample(s)
+    fb = qcb.GaugeField(ctx, dims)
+    fb.set_links(u)
+    b = qcb.EventChains(fb, BASE, 41)
+    b.sample_n(shifts)
+    ra, ca = a.chains()
+    rb, cb = b.chains()
+    assert ca == cb == 3
+    assert np.array_equal(ra, rb)
+    assert np.array_equal(fa.get_links(), fb.get_links())
+    for o in (a, b, fa, fb):
+        o.close()
