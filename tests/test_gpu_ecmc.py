@@ -31,10 +31,13 @@ def _compare(rec, ref, tol=1e-9):
         assert np.abs(rec[k] - ref[k]).max() < tol, k
 
 
-@pytest.mark.parametrize("dims,l,poisson,beta", [((8, 8, 8, 8), 4, 0, 6.0), ((6, 6, 12, 6), 3, 1, 5.7),
-                                                ((8, 8, 8, 16), 4, 0, 2.0)])
-def test_matches_oracle_event_for_event(ctx, dims, l, poisson, beta):
-    p = dict(BASE, l_core=l, poisson=poisson, beta=beta)
+@pytest.mark.parametrize("dims,l,poisson,beta,eps_set", [((8, 8, 8, 8), 4, 0, 6.0, 0.15),
+                                                        ((6, 6, 12, 6), 3, 1, 5.7, 0.15),
+                                                        ((8, 8, 8, 16), 4, 0, 2.0, 0.15),
+                                                        ((10, 10, 10, 10), 5, 0, 6.2, 0.3),
+                                                        ((8, 8, 8, 8), 4, 1, 6.0, 0.0)])
+def test_matches_oracle_event_for_event(ctx, dims, l, poisson, beta, eps_set):
+    p = dict(BASE, l_core=l, poisson=poisson, beta=beta, epsilon_set=eps_set)
     u = orc.hot_philox(dims, 21)
     f = qcb.GaugeField(ctx, dims)
     f.set_links(u)

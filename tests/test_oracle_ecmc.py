@@ -87,7 +87,7 @@ def _frozen_mask(dims, l, cum):
     return m
 
 
-@pytest.mark.parametrize("dims,l,poisson", [((8, 8, 8, 8), 4, 0), ((6, 9, 6, 3), 3, 1)])
+@pytest.mark.parametrize("dims,l,poisson", [((8, 8, 8, 8), 4, 0), ((6, 9, 6, 3), 3, 1), ((10, 5, 5, 10), 5, 0)])
 def test_blocks_frozen_links_and_confinement(dims, l, poisson):
     p = dict(PARAMS, l_core=l, poisson=poisson)
     u = orc.hot_philox(dims, 5)
