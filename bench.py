@@ -506,6 +506,7 @@ def ecmc_section(ctx, steps=5, warmup=3, cpu_budget_s=8.0, cpu=True):
     out = {"metric": "ECMC events/s (one link update each)", "value": rate, "unit": "events/s",
            "workload": f"{ECMC_L}^4 fp64, {ch.n_chains} chains of {ECMC_LCORE}^4 blocks, beta={BETA}, theta_sample="
                        f"{ECMC_THETA:g}, refresh 50/15, epsilon_set 0.15",
+           "lanes_per_chain": ch.lanes,
            "ms_per_step": ms / steps, "events_per_chain_per_step": events / steps / ch.n_chains,
            "lambda": ECMC_THETA * ch.n_chains * steps / lifts, "same_site_lift_frac": revs / lifts,
            "plaquette": plaq, "gpu_launches": launches,
@@ -524,21 +525,25 @@ def ecmc_section(ctx, steps=5, warmup=3, cpu_budget_s=8.0, cpu=True):
     return out
 
 
-def ecmc_profile_case(ctx):
+def ecmc_profile_case(ctx, lanes=3):
     """The small case an ncu capture of k_ecmc_sample runs on (a few GB on the device): a 42^4
-    FP64 lattice as 14^4 blocks of 3^4 (38416 chains, a full wave of resident chains), Haar
-    hot start + 5 heatbath sweeps, two sample calls (capture the second: -s 1 -c 1)."""
+    FP64 lattice as 14^4 blocks of 3^4 (38416 chains), Haar hot start + 5 heatbath sweeps, two
+    sample calls (capture the second: -s 1 -c 1).  Three lanes per chain is the kernel shape the
+    library picks for the 64^4 workload's 65536 chains; with one, the thread counters count each
+    operation of the algorithm once (the chains take the same events at any lane count)."""
     import qcb
 
     f = qcb.GaugeField(ctx, (42,) * 4, "fp64", 18)
     f.hot_start(1)
     qcb._lib.check(qcb._lib.lib().qcb_heatbath(f.h, BETA, 5, 1, 3, 0))
     ch = qcb.EventChains(f, qcb.ecmc.params(beta=BETA, theta_sample=ECMC_THETA, l_core=3), 7)
+    ch.lanes = lanes
     ch.sample((0, 1, 2, 0))
     ch.counters(reset=True)
     ch.sample((1, 1, 0, 2))
     events, lifts, revs = ch.counters(reset=True)
-    out = {"case": "ecmc 42^4 l_core 3", "chains": ch.n_chains, "events_second_call": events, "lifts": lifts}
+    out = {"case": "ecmc 42^4 l_core 3", "chains": ch.n_chains, "lanes_per_chain": ch.lanes,
+           "events_second_call": events, "lifts": lifts}
     ch.close()
     f.close()
     return out
@@ -817,6 +822,9 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="run only warmup + steps of the workload (for ncu); print launch counts")
     ap.add_argument("--storage", choices=["fp32-12", "fp64-18"], default="fp32-12")
+    ap.add_argument("--ecmc-lanes", type=int, choices=[1, 3, 6], default=3,
+                    help="lanes per chain of the event-chain profile case (1: no lane repeats the "
+                         "chain's serial work, so thread counters count the algorithm's operations)")
     ap.add_argument("--workload", choices=["precision", "large", "batch", "ecmc"], default="precision",
                     help="large: the 64^4 single-lattice workload; batch: the 64-lattice batching workload "
                          "alone; ecmc: the event-chain workload alone; each printed as its own JSON object")
@@ -871,7 +879,7 @@ def main():
 
             ctx = qcb.Context(0)
             if args.profile:
-                print(json.dumps(ecmc_profile_case(ctx)))
+                print(json.dumps(ecmc_profile_case(ctx, args.ecmc_lanes)))
             else:
                 print(json.dumps(ecmc_section(ctx, steps=args.steps, warmup=args.warmup,
                                               cpu=not args.no_cpu_baseline)))

@@ -18,6 +18,7 @@ struct qcb_ecmc {
   uint64_t calls = 0;  // sample calls made (the key of the next call's set)
   int nb[4] = {0, 0, 0, 0};
   uint32_t n_chains = 0;
+  int lanes = 0;               // lanes per chain asked for (0: chosen by the library)
   double2* d_links = nullptr;  // FP64 array-of-structures copy of the lattice
   double2* d_set = nullptr;
   qcb_ecmc_chain* d_chains = nullptr;
@@ -124,6 +125,21 @@ int qcb_ecmc_num_chains(const qcb_ecmc* e, int* n) {
   return QCB_OK;
 }
 
+int qcb_ecmc_set_lanes(qcb_ecmc* e, int lanes) {
+  if (!e) return efail(QCB_ERR_INVALID, "null argument");
+  if (lanes != 0 && lanes != 1 && lanes != 3 && lanes != 6)
+    return efail(QCB_ERR_INVALID, "lanes per chain must be 0 (automatic), 1, 3 or 6");
+  e->lanes = lanes;
+  return QCB_OK;
+}
+
+int qcb_ecmc_lanes(const qcb_ecmc* e, int* lanes) {
+  if (!e || !lanes) return efail(QCB_ERR_INVALID, "null argument");
+  const int layout = ecmc_layout(e->n_chains, e->lanes);
+  *lanes = layout == ECMC_LAYOUT_1 ? 1 : (layout == ECMC_LAYOUT_6 || layout == ECMC_LAYOUT_6C ? 6 : 3);
+  return QCB_OK;
+}
+
 int qcb_ecmc_sample_n(qcb_ecmc* e, const int* shifts, int n) {
   if (!e || (!shifts && n > 0)) return efail(QCB_ERR_INVALID, "null argument");
   if (n < 0) return efail(QCB_ERR_INVALID, "negative call count");
@@ -156,7 +172,7 @@ int qcb_ecmc_sample_n(qcb_ecmc* e, const int* shifts, int n) {
   for (int k = 0; k < n; ++k) {
     for (int d = 0; d < 4; ++d) a.cum[d] = ((shifts[4 * k + d] % a.L[d]) + a.L[d]) % a.L[d];
     ECU(launch_ecmc_set(e->d_set, e->p.epsilon_set, e->seed, e->calls, c->stream), "ECMC set");
-    ECU(launch_ecmc_sample(a, c->stream, 0), "ECMC sample");
+    ECU(launch_ecmc_sample(a, ecmc_layout(e->n_chains, e->lanes), c->stream), "ECMC sample");
     c->launches += 2;
     e->calls++;
   }

@@ -29,7 +29,15 @@ struct EcmcLaunch {
 
 // The call's set, drawn from Philox counters (j, call_lo, call_hi, set domain).
 cudaError_t launch_ecmc_set(double2* set, double epsilon, uint64_t seed, uint64_t call, cudaStream_t s);
-cudaError_t launch_ecmc_sample(const EcmcLaunch& a, cudaStream_t s, int block);
+// Launch shapes of the sample kernel: lanes per chain (1, 3 or 6, each lane computing an
+// equal share of the six staples; lanes 0-2 of a group also share the lift's three products)
+// and the register budget (C: capped for more resident chains).  All give the same results,
+// bit for bit.
+enum { ECMC_LAYOUT_1 = 1, ECMC_LAYOUT_3 = 3, ECMC_LAYOUT_3C = 4, ECMC_LAYOUT_6 = 6, ECMC_LAYOUT_6C = 7 };
+// The layout for n_chains chains: `lanes` 1, 3 or 6 fixes the lanes per chain, 0 lets the
+// number of chains choose them too; the register budget follows the waves of resident chains.
+int ecmc_layout(uint32_t n_chains, int lanes);
+cudaError_t launch_ecmc_sample(const EcmcLaunch& a, int layout, cudaStream_t s);
 // out[0..2] += the chains' events, lifts, same-site lifts; zeroes them with reset.
 cudaError_t launch_ecmc_counters(qcb_ecmc_chain* chains, uint32_t n, unsigned long long* out, int reset,
                                  cudaStream_t s);

@@ -1,5 +1,5 @@
 // k_ecmc.cu — event-chain Monte Carlo: every l_core^4 block runs its own persistent chain,
-// one thread per chain, all chains of the lattice in one launch.
+// on one, three or six lanes of a warp, all chains of the lattice in one launch.
 //
 // The reference runs one chain per MPI rank (mpi::ecmccb::sample_persistant,
 // src/ecmc/ecmc_mpi_cb.cpp:496-637) on a padded block whose halo and low faces are frozen
@@ -29,9 +29,23 @@ namespace {
 constexpr uint32_t ECMC_CHAIN = 0xECEC0001u, ECMC_SET = 0xECEC0002u;
 constexpr uint64_t ECMC_MAX_EVENTS = 1ull << 26;
 constexpr double PI = 3.141592653589793;  // the double nearest pi
+// Sample kernel blocks: two warps.  Register caps: none (255 per thread), or ECMC_CAPPED
+// blocks of 64 threads per SM (168 per thread).
+constexpr int ECMC_WARPS = 2, ECMC_CAPPED = 6;
 
 typedef m3<double> M;
 typedef cx<double> Z;
+
+// The file is compiled without automatic contraction (-fmad=false) and the products of the
+// event loop use these explicit fused multiply-adds, so that every instantiation of the
+// sample kernel (one, three or six lanes per chain) rounds every operation the same way.
+__device__ __forceinline__ Z cmul(Z a, Z b) { return mk(fma(a.re, b.re, -(a.im * b.im)), fma(a.re, b.im, a.im * b.re)); }
+// acc + a b
+__device__ __forceinline__ Z cfma(Z a, Z b, Z acc) {
+  return mk(fma(a.re, b.re, fma(-a.im, b.im, acc.re)), fma(a.re, b.im, fma(a.im, b.re, acc.im)));
+}
+// a0 b0 + a1 b1 + a2 b2
+__device__ __forceinline__ Z cdot3(Z a0, Z b0, Z a1, Z b1, Z a2, Z b2) { return cfma(a2, b2, cfma(a1, b1, cmul(a0, b0))); }
 
 // Uniform in (0, 1) from two 32-bit words: (top 53 bits of hi:lo + 1/2) 2^-53.
 __device__ __forceinline__ double u53(uint32_t lo, uint32_t hi) {
@@ -103,17 +117,6 @@ __device__ __noinline__ M haar(Stream& g) {
     n[2 * k + 1] = rad * sn;
   }
   return haar_from_normals(n);
-}
-
-__device__ __forceinline__ M ld(const double2* links, uint32_t s, int mu) {
-  const double2* q = links + ((size_t)s * 4 + (size_t)mu) * 9;
-  M u;
-#pragma unroll
-  for (int c = 0; c < 9; ++c) {
-    const double2 v = q[c];
-    u.e[c / 3][c % 3] = mk(v.x, v.y);
-  }
-  return u;
 }
 
 // The block of one chain: local coordinates lc (in [-1, l] for every link a chain at an
@@ -216,12 +219,7 @@ __device__ __forceinline__ void ld_row(const double2* L, uint32_t s, int mu, int
 // out_c = sum_a v_a M_ac
 __device__ __forceinline__ void vmul(const Z v[3], const M& m, Z out[3]) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) out[c] = v[0] * m.e[0][c] + v[1] * m.e[1][c] + v[2] * m.e[2][c];
-}
-// out_c = sum_a v_a conj(M_ca)  (v times M^+)
-__device__ __forceinline__ void vmul_a(const Z v[3], const M& m, Z out[3]) {
-#pragma unroll
-  for (int c = 0; c < 3; ++c) out[c] = v[0] * conj(m.e[c][0]) + v[1] * conj(m.e[c][1]) + v[2] * conj(m.e[c][2]);
+  for (int c = 0; c < 3; ++c) out[c] = cdot3(v[0], m.e[0][c], v[1], m.e[1][c], v[2], m.e[2][c]);
 }
 // Q_km of the Hermitian Q
 __device__ __forceinline__ Z qel(const Herm& q, int k, int m) {
@@ -235,7 +233,7 @@ __device__ __forceinline__ double im_row_q(const Z r[3], const Herm& q, int m) {
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const Z a = qel(q, k, m);
-    s += r[k].re * a.im + r[k].im * a.re;
+    s = fma(r[k].re, a.im, fma(r[k].im, a.re, s));
   }
   return s;
 }
@@ -251,19 +249,6 @@ __device__ __forceinline__ int lift_link(int i, bool fwd, const int lc[4], int m
     case 2: shifted(lc, nu, fwd ? 1 : -1, -1, 0, out); return mu;
     default: shifted(lc, fwd ? -1 : nu, fwd ? 0 : -1, -1, 0, out); return nu;
   }
-}
-
-// U or U^+ by a flag, element by element (no branch).
-__device__ __forceinline__ M cdag(const M& u, bool dag) {
-  M r;
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      const Z a = u.e[i][j], b = u.e[j][i];
-      r.e[i][j] = dag ? mk(b.re, -b.im) : a;
-    }
-  return r;
 }
 
 // Q = R diag(1, -1, 0) R^dagger from columns 0 and 1 of R.
@@ -283,67 +268,58 @@ __device__ __forceinline__ Herm ds_matrix_cols(const Z c0[3], const Z c1[3]) {
 // P of each link of the reference is a cyclic rotation rot_s = F_s F_s+1 F_s+2 F_s+3 or the
 // adjoint of one, so every dS is +-Im tr(Q rot_s) for s = 0, 3 and X (1 forward, 2 backward):
 // forward P0 = rot0, P1 = rot1, P2 = rot3^+, P3 = rot0^+; backward P0 = rot0, P1 = rot2^+,
-// P2 = rot3^+, P3 = rot3.  The traces against the current Q and the proposal's Qn take
-// seven SU(3) products, row-streamed; only rot_X depends on the orientation.  Not inlined:
-// the products would otherwise share the event loop's register budget.
-struct LiftTraces {
-  double t0, t3, tx, n0, n3, nx;
+// P2 = rot3^+, P3 = rot3.  One call forms one rot_s as (F_s F_s+1)(F_s+2 F_s+3), by rows,
+// and returns (Im tr(Q rot_s), Im tr(Qn rot_s)) for the current Q and the proposal's Qn.
+// With several lanes per chain, lanes 0, 1, 2 form rot0, rotX, rot3 at once; with one, the
+// lane makes the three calls in turn: the same operations either way.  Not inlined: the
+// products would otherwise share the event loop's register budget.
+struct Factor {
+  uint32_t site;
+  int dir;
+  bool dag;
 };
-__device__ __noinline__ LiftTraces lift_traces(const double2* L, uint32_t x, uint32_t s1, uint32_t s2, uint32_t s3,
-                                               int mu, int nu, bool fwd, Herm q, Herm qn) {
-  LiftTraces t = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  const M B = mul_an(ld(L, s2, mu), cdag(ld(L, s3, nu), fwd));  // F2 F3
-  const M F1 = cdag(ld(L, s1, nu), !fwd);
-  // rot0 = F0 F1 (F2 F3), by rows of F0
+__device__ __forceinline__ Factor lift_factor(int f, uint32_t x, uint32_t s1, uint32_t s2, uint32_t s3, int mu, int nu,
+                                              bool fwd) {
+  f &= 3;
+  Factor r;
+  r.site = f == 0 ? x : (f == 1 ? s1 : (f == 2 ? s2 : s3));
+  r.dir = (f & 1) ? nu : mu;
+  r.dag = f == 0 ? false : (f == 1 ? !fwd : (f == 2 ? true : fwd));
+  return r;
+}
+// row m of F (U, or U^+ whose row m is the conjugated column m of U)
+__device__ __forceinline__ void ld_row_f(const double2* L, const Factor& f, int m, Z out[3]) {
+  const double2* q = L + ((size_t)f.site * 4 + (size_t)f.dir) * 9;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double2 v = q[f.dag ? 3 * c + m : 3 * m + c];
+    out[c] = mk(v.x, f.dag ? -v.y : v.y);
+  }
+}
+__device__ __noinline__ double2 lift_trace_lane(const double2* L, Factor fa, Factor fb, Factor fc, Factor fd, Herm q,
+                                                Herm qn) {
+  M D, P, B;
+#pragma unroll
+  for (int m = 0; m < 3; ++m) ld_row_f(L, fd, m, D.e[m]);
 #pragma unroll
   for (int m = 0; m < 3; ++m) {
-    Z u[3], a[3], r[3];
-    ld_row(L, x, mu, m, u);
-    vmul(u, F1, a);
-    vmul(a, B, r);
-    t.t0 += im_row_q(r, q, m);
-    t.n0 += im_row_q(r, qn, m);
+    Z r[3];
+    ld_row_f(L, fc, m, r);
+    vmul(r, D, P.e[m]);
   }
-  if (fwd) {  // rot1 = F1 (F2 F3) F0, by rows of F1
-    const M U0 = ld(L, x, mu);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-      Z a[3], r[3];
-      vmul(F1.e[m], B, a);
-      vmul(a, U0, r);
-      t.tx += im_row_q(r, q, m);
-      t.nx += im_row_q(r, qn, m);
-    }
-  } else {  // rot2 = (F2 F3)(F0 F1), by rows of F2 F3
-    const M A = mul_nn(ld(L, x, mu), F1);
+  for (int m = 0; m < 3; ++m) ld_row_f(L, fb, m, B.e[m]);
+  double t = 0.0, n = 0.0;
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-      Z r[3];
-      vmul(B.e[m], A, r);
-      t.tx += im_row_q(r, q, m);
-      t.nx += im_row_q(r, qn, m);
-    }
+  for (int m = 0; m < 3; ++m) {
+    Z r[3], u[3], w[3];
+    ld_row_f(L, fa, m, r);
+    vmul(r, B, u);
+    vmul(u, P, w);
+    t += im_row_q(w, q, m);
+    n += im_row_q(w, qn, m);
   }
-  // rot3 = F3 (F0 F1) F2, by rows of F3 (row m of U3^+ is the conjugated column m of U3)
-  {
-    const M A = mul_nn(ld(L, x, mu), F1);
-    const M U2 = ld(L, s2, mu);
-    const double2* u3 = L + ((size_t)s3 * 4 + (size_t)nu) * 9;
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {
-      Z f[3], a[3], r[3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const double2 v = u3[fwd ? 3 * c + m : 3 * m + c];
-        f[c] = mk(v.x, fwd ? -v.y : v.y);
-      }
-      vmul(f, A, a);
-      vmul_a(a, U2, r);
-      t.t3 += im_row_q(r, q, m);
-      t.n3 += im_row_q(r, qn, m);
-    }
-  }
-  return t;
+  return make_double2(t, n);
 }
 
 // su2_quaternion_to_su3 (src/su3/utils.cpp:33-45) of (x0, x1, x2, x3) in subgroup (i, j).
@@ -402,10 +378,19 @@ __global__ void k_ecmc_set(double2* set, double eps, uint32_t k0, uint32_t k1, u
 }
 
 // sample_persistant (ecmc_mpi_cb.cpp:496-637) for chain c: events until it has travelled
-// theta_sample; the chain record persists across calls.
-__global__ void __launch_bounds__(64) k_ecmc_sample(EcmcLaunch a) {
-  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.n_chains) return;
+// theta_sample; the chain record persists across calls.  GROUP lanes of one warp (1, 3 or
+// 6) run a chain together: each computes its share of the six staples and, with three or
+// more, lanes 0-2 one product each of a lift; all of them carry the chain's state and take
+// the same branches, so the group never diverges.  Every lane stores the updated link (the
+// same values), so each lane's later loads see its own stores and no barrier is needed.
+template <int GROUP, int MINB>
+__global__ void __launch_bounds__(ECMC_WARPS * 32, MINB) k_ecmc_sample(EcmcLaunch a) {
+  static_assert(GROUP == 1 || GROUP == 3 || GROUP == 6, "a chain's lanes split its six staples evenly");
+  constexpr int PER_WARP = 32 / GROUP;  // chains per warp; 32 % GROUP lanes stay idle
+  const int lane = threadIdx.x & 31, slot = lane / GROUP, sub = lane - slot * GROUP, lane0 = slot * GROUP;
+  const uint32_t c = (blockIdx.x * ECMC_WARPS + (threadIdx.x >> 5)) * PER_WARP + slot;
+  if (slot >= PER_WARP || c >= a.n_chains) return;
+  const unsigned gmask = GROUP == 1 ? (1u << lane) : (((1u << GROUP) - 1u) << lane0);
   qcb_ecmc_chain& rec = a.chains[c];
   Block blk;
   blk.l = a.l;
@@ -477,79 +462,93 @@ __global__ void __launch_bounds__(64) k_ecmc_sample(EcmcLaunch a) {
       ld_row(links, x, mu, c, ur);
 #pragma unroll
       for (int j2 = 0; j2 < 3; ++j2) {
-        T.e[0][j2] = T.e[0][j2] + conj(R.e[c][0]) * ur[j2];
-        T.e[1][j2] = T.e[1][j2] + conj(R.e[c][1]) * ur[j2];
+        T.e[0][j2] = cfma(conj(R.e[c][0]), ur[j2], T.e[0][j2]);
+        T.e[1][j2] = cfma(conj(R.e[c][1]), ur[j2], T.e[1][j2]);
       }
     }
     // compute_list_staples (ecmc_mpi_cb.cpp:12-36): for each nu != mu, forward then backward;
-    // the first minimum of the six reject angles
+    // lane `sub` of the chain's group computes staples sub, sub + GROUP, ...; the angles are
+    // then taken in staple order, keeping the first minimum.  Staple k draws the event's
+    // uniform number k.
     double best = 0.0;
     int j = 0;
 #pragma unroll 1
-    for (int k = 0; k < 6; ++k) {
+    for (int t = 0; t < 6 / GROUP; ++t) {
+      const int k = sub + t * GROUP;
       const int nu = (k >> 1) + ((k >> 1) >= mu ? 1 : 0);
-      int p[4], q[4];
-      Z P00 = mk(0.0, 0.0), P11 = mk(0.0, 0.0);
-      if ((k & 1) == 0) {  // S = X W^+, X = U_nu(x+mu), W = U_nu(x) U_mu(x+nu)
-        shifted(lc, mu, 1, -1, 0, p);
-        shifted(lc, nu, 1, -1, 0, q);
-        // v_k = (W^+ R)_k0 and (W^+ R)_k1, by rows of W
-        Z v0[3] = {mk(0.0, 0.0), mk(0.0, 0.0), mk(0.0, 0.0)}, v1[3] = {v0[0], v0[1], v0[2]};
-        {
-          const M C = ld(links, blk.site(q), mu);
+      const bool fwd = (k & 1) == 0;
+      // Forward S = X W^+ (X = U_nu(x+mu), W = U_nu(x) U_mu(x+nu)); backward S = W^+ D
+      // (W = U_mu(x-nu) U_nu(x+mu-nu), D = U_nu(x-nu)).  With E = X or D, Tt = T E forward or
+      // T backward, and (E'R) = R forward or D R backward, both are
+      // P_ii = sum_r (Tt W^+)_ir (E'R)_ri, and (Tt W^+)_ir = sum_m conj(W1_rm) (Tt W2^+)_im
+      // for W = W1 W2: one code path for both orientations, streaming every link by rows.
+      int q4[4];
+      shifted(lc, fwd ? mu : nu, fwd ? 1 : -1, -1, 0, q4);
+      const uint32_t se = blk.site(q4);
+      shifted(lc, nu, fwd ? 1 : -1, fwd ? -1 : mu, fwd ? 0 : 1, q4);
+      const uint32_t s2 = blk.site(q4);
+      const int d2 = fwd ? mu : nu;
+      shifted(lc, nu, fwd ? 0 : -1, -1, 0, q4);
+      const uint32_t s1 = blk.site(q4);
+      const int d1 = fwd ? nu : mu;
+      // With one lane per chain every lane of a warp is at the same staple, so the orientation
+      // is a branch; with more, the two orientations run as one instruction stream.
+      const bool fwd_math = GROUP == 1 ? fwd : true;
+      Z g0[3], g1[3];  // rows 0 and 1 of Tt
+      if (fwd_math) {
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            Z b[3], w[3];
-            ld_row(links, x, nu, c, b);
-            vmul(b, C, w);
+        for (int c2 = 0; c2 < 3; ++c2) g0[c2] = g1[c2] = mk(0.0, 0.0);
 #pragma unroll
-            for (int kk = 0; kk < 3; ++kk) {
-              v0[kk] = v0[kk] + conj(w[kk]) * R.e[c][0];
-              v1[kk] = v1[kk] + conj(w[kk]) * R.e[c][1];
-            }
+        for (int r = 0; r < 3; ++r) {
+          Z er[3];
+          ld_row(links, se, nu, r, er);
+#pragma unroll
+          for (int c2 = 0; c2 < 3; ++c2) {
+            const Z e = fwd ? er[c2] : mk(r == c2 ? 1.0 : 0.0, 0.0);
+            g0[c2] = cfma(T.e[0][r], e, g0[c2]);
+            g1[c2] = cfma(T.e[1][r], e, g1[c2]);
           }
         }
-        // y_i = T_i. X, by rows of X
-        Z y0[3] = {mk(0.0, 0.0), mk(0.0, 0.0), mk(0.0, 0.0)}, y1[3] = {y0[0], y0[1], y0[2]};
-        const uint32_t sp = blk.site(p);
+      } else {
 #pragma unroll
-        for (int a2 = 0; a2 < 3; ++a2) {
-          Z xr[3];
-          ld_row(links, sp, nu, a2, xr);
-#pragma unroll
-          for (int kk = 0; kk < 3; ++kk) {
-            y0[kk] = y0[kk] + T.e[0][a2] * xr[kk];
-            y1[kk] = y1[kk] + T.e[1][a2] * xr[kk];
-          }
-        }
-#pragma unroll
-        for (int kk = 0; kk < 3; ++kk) {
-          P00 = P00 + y0[kk] * v0[kk];
-          P11 = P11 + y1[kk] * v1[kk];
-        }
-      } else {  // S = W^+ D, W = U_mu(x-nu) U_nu(x+mu-nu), D = U_nu(x-nu)
-        shifted(lc, mu, 1, nu, -1, p);
-        shifted(lc, nu, -1, -1, 0, q);
-        const uint32_t sq = blk.site(q);
-        const M C = ld(links, blk.site(p), nu);
-        // P_ii = sum_k (T_i. W^+)_k (D R)_ki, by rows k of W and of D
-#pragma unroll
-        for (int kk = 0; kk < 3; ++kk) {
-          Z b[3], w[3], d[3];
-          ld_row(links, sq, mu, kk, b);
-          vmul(b, C, w);
-          const Z y0 = T.e[0][0] * conj(w[0]) + T.e[0][1] * conj(w[1]) + T.e[0][2] * conj(w[2]);
-          const Z y1 = T.e[1][0] * conj(w[0]) + T.e[1][1] * conj(w[1]) + T.e[1][2] * conj(w[2]);
-          ld_row(links, sq, nu, kk, d);
-          const Z z0 = d[0] * R.e[0][0] + d[1] * R.e[1][0] + d[2] * R.e[2][0];
-          const Z z1 = d[0] * R.e[0][1] + d[1] * R.e[1][1] + d[2] * R.e[2][1];
-          P00 = P00 + y0 * z0;
-          P11 = P11 + y1 * z1;
-        }
+        for (int c2 = 0; c2 < 3; ++c2) g0[c2] = T.e[0][c2], g1[c2] = T.e[1][c2];
       }
-      const double rej = reject_from(P00, P11, a.beta, -log(g.uni()), eps);
-      if (k == 0 || rej < best) best = rej, j = k;
+      Z h0[3], h1[3];  // rows 0 and 1 of Tt W2^+
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        Z w2[3];
+        ld_row(links, s2, d2, m, w2);
+        h0[m] = cdot3(g0[0], conj(w2[0]), g0[1], conj(w2[1]), g0[2], conj(w2[2]));
+        h1[m] = cdot3(g1[0], conj(w2[0]), g1[1], conj(w2[1]), g1[2], conj(w2[2]));
+      }
+      Z P00 = mk(0.0, 0.0), P11 = mk(0.0, 0.0);
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        Z w1[3];
+        ld_row(links, s1, d1, r, w1);
+        const Z y0 = cdot3(conj(w1[0]), h0[0], conj(w1[1]), h0[1], conj(w1[2]), h0[2]);
+        const Z y1 = cdot3(conj(w1[0]), h1[0], conj(w1[1]), h1[1], conj(w1[2]), h1[2]);
+        Z z0 = R.e[r][0], z1 = R.e[r][1];
+        if (GROUP > 1 || !fwd) {
+          Z er[3];
+          ld_row(links, se, nu, r, er);
+          const Z e0 = cdot3(er[0], R.e[0][0], er[1], R.e[1][0], er[2], R.e[2][0]);
+          const Z e1 = cdot3(er[0], R.e[0][1], er[1], R.e[1][1], er[2], R.e[2][1]);
+          z0 = fwd ? z0 : e0;
+          z1 = fwd ? z1 : e1;
+        }
+        P00 = cfma(y0, z0, P00);
+        P11 = cfma(y1, z1, P11);
+      }
+      const double rej = reject_from(P00, P11, a.beta, -log(chain_uniform(g.chain, g.k0, g.k1, g.n + k)), eps);
+#pragma unroll
+      for (int q = 0; q < GROUP; ++q) {
+        const double rq = GROUP == 1 ? rej : __shfl_sync(gmask, rej, lane0 + q);
+        const int kq = t * GROUP + q;
+        if (kq == 0 || rq < best) best = rq, j = kq;
+      }
     }
+    g.n += 6;
     const double d_sample = theta_sample - tr_sample;
     const double d_site = th_site - tr_site;
     const double d_R = th_R - tr_R;
@@ -574,16 +573,16 @@ __global__ void __launch_bounds__(64) k_ecmc_sample(EcmcLaunch a) {
         Z ur[3];
         ld_row(links, x, mu, c, ur);
 #pragma unroll
-        for (int j2 = 0; j2 < 3; ++j2) t2[j2] = t2[j2] + conj(R.e[c][2]) * ur[j2];
+        for (int j2 = 0; j2 < 3; ++j2) t2[j2] = cfma(conj(R.e[c][2]), ur[j2], t2[j2]);
       }
       const Z ep = mk(cs, sn), em = mk(cs, -sn);
       double2* q = links + ((size_t)x * 4 + (size_t)mu) * 9;
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
-        const Z r0 = R.e[i][0] * ep, r1 = R.e[i][1] * em, r2 = R.e[i][2];
+        const Z r0 = cmul(R.e[i][0], ep), r1 = cmul(R.e[i][1], em), r2 = R.e[i][2];
 #pragma unroll
         for (int j2 = 0; j2 < 3; ++j2) {
-          const Z v = r0 * T.e[0][j2] + r1 * T.e[1][j2] + r2 * t2[j2];
+          const Z v = cdot3(r0, T.e[0][j2], r1, T.e[1][j2], r2, t2[j2]);
           q[3 * i + j2] = make_double2(v.re, v.im);
         }
       }
@@ -637,17 +636,42 @@ __global__ void __launch_bounds__(64) k_ecmc_sample(EcmcLaunch a) {
         for (int m = 0; m < 3; ++m) {
           const double2 s0 = sq[3 * m], s1v = sq[3 * m + 1], s2v = sq[3 * m + 2];
           const Z a0 = mk(s0.x, s0.y), a1 = mk(s1v.x, s1v.y), a2 = mk(s2v.x, s2v.y);
-          c0[m] = a0 * R.e[0][0] + a1 * R.e[1][0] + a2 * R.e[2][0];
-          c1[m] = a0 * R.e[0][1] + a1 * R.e[1][1] + a2 * R.e[2][1];
+          c0[m] = cdot3(a0, R.e[0][0], a1, R.e[1][0], a2, R.e[2][0]);
+          c1[m] = cdot3(a0, R.e[0][1], a1, R.e[1][1], a2, R.e[2][1]);
         }
         Qn = ds_matrix_cols(c0, c1);
       }
-      const LiftTraces tr = lift_traces(links, x, s1, s2, s3, mu, nu, fwd, ds_matrix(R), Qn);
+      // traces of rot0, rotX, rot3 against Q (tq) and Qn (tn)
+      double tq[3], tn[3];
+      const Herm Q = ds_matrix(R);
+      if (GROUP >= 3) {
+        const int i3 = sub % 3, r0 = i3 == 0 ? 0 : (i3 == 1 ? (fwd ? 1 : 2) : 3);
+        const double2 v = lift_trace_lane(links, lift_factor(r0, x, s1, s2, s3, mu, nu, fwd),
+                                          lift_factor(r0 + 1, x, s1, s2, s3, mu, nu, fwd),
+                                          lift_factor(r0 + 2, x, s1, s2, s3, mu, nu, fwd),
+                                          lift_factor(r0 + 3, x, s1, s2, s3, mu, nu, fwd), Q, Qn);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          tq[q] = __shfl_sync(gmask, v.x, lane0 + q);
+          tn[q] = __shfl_sync(gmask, v.y, lane0 + q);
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const int r0 = q == 0 ? 0 : (q == 1 ? (fwd ? 1 : 2) : 3);
+          const double2 v = lift_trace_lane(links, lift_factor(r0, x, s1, s2, s3, mu, nu, fwd),
+                                            lift_factor(r0 + 1, x, s1, s2, s3, mu, nu, fwd),
+                                            lift_factor(r0 + 2, x, s1, s2, s3, mu, nu, fwd),
+                                            lift_factor(r0 + 3, x, s1, s2, s3, mu, nu, fwd), Q, Qn);
+          tq[q] = v.x;
+          tn[q] = v.y;
+        }
+      }
       // dS of each candidate (0 for frozen links) under R and under R_new
-      const double ds0 = tr.t0, dn0 = tr.n0;
-      const double ds1 = f1 ? 0.0 : (fwd ? tr.tx : -tr.tx), dn1 = fwd ? tr.nx : -tr.nx;
-      const double ds2 = f2 ? 0.0 : -tr.t3, dn2 = -tr.n3;
-      const double ds3 = f3 ? 0.0 : (fwd ? -tr.t0 : tr.t3), dn3 = fwd ? -tr.n0 : tr.n3;
+      const double ds0 = tq[0], dn0 = tn[0];
+      const double ds1 = f1 ? 0.0 : (fwd ? tq[1] : -tq[1]), dn1 = fwd ? tn[1] : -tn[1];
+      const double ds2 = f2 ? 0.0 : -tq[2], dn2 = -tn[2];
+      const double ds3 = f3 ? 0.0 : (fwd ? -tq[0] : tq[2]), dn3 = fwd ? -tn[0] : tn[2];
       const double a0 = fabs(ds0), a1 = fabs(ds1), a2 = fabs(ds2), a3 = fabs(ds3);
       const double sum = a0 + a1 + a2 + a3;
       const double p0 = a0 / sum, p1 = a1 / sum, p2 = a2 / sum;
@@ -678,6 +702,7 @@ __global__ void __launch_bounds__(64) k_ecmc_sample(EcmcLaunch a) {
       eps = new_eps;
     }
   }
+  if (sub != 0) return;
 #pragma unroll
   for (int d = 0; d < 4; ++d) rec.site[d] = lc[d];
   rec.mu = mu;
@@ -731,10 +756,67 @@ cudaError_t launch_ecmc_set(double2* set, double epsilon, uint64_t seed, uint64_
   return cudaGetLastError();
 }
 
-cudaError_t launch_ecmc_sample(const EcmcLaunch& a, cudaStream_t s, int block) {
-  if (block <= 0 || block > 64) block = 64;
-  k_ecmc_sample<<<(a.n_chains + block - 1) / block, block, 0, s>>>(a);
+namespace {
+
+template <int GROUP, int MINB>
+cudaError_t launch_sample(const EcmcLaunch& a, cudaStream_t s) {
+  const uint32_t per_block = ECMC_WARPS * (32 / GROUP);
+  k_ecmc_sample<GROUP, MINB><<<(a.n_chains + per_block - 1) / per_block, ECMC_WARPS * 32, 0, s>>>(a);
   return cudaGetLastError();
+}
+
+// Chains resident on the device at once for the kernel of GROUP lanes per chain.
+template <int GROUP, int MINB>
+uint32_t resident_chains() {
+  int dev = 0, sms = 0, blocks = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_ecmc_sample<GROUP, MINB>, ECMC_WARPS * 32, 0) !=
+          cudaSuccess)
+    return 0;
+  return (uint32_t)sms * (uint32_t)blocks * ECMC_WARPS * (32 / GROUP);
+}
+
+}  // namespace
+
+// A call lasts about as long as its number of waves of resident chains, each chain taking a
+// similar number of events, so shape k is expected to run at rate_k n / (cap_k ceil(n / cap_k)),
+// rate_k being its event rate with the device full.  The rates are the ones measured on B200
+// (1e8 events/s, reference default budgets, 8192 to 65536 chains); the capacities come from
+// the occupancy calculator.  Among equal estimates the earlier shape wins.
+int ecmc_layout(uint32_t n_chains, int lanes) {
+  struct Shape {
+    int layout, lanes;
+    uint32_t cap;
+    double rate;
+  };
+  static const Shape shapes[] = {
+      {ECMC_LAYOUT_6, 6, resident_chains<6, 1>(), 2.9},
+      {ECMC_LAYOUT_6C, 6, resident_chains<6, ECMC_CAPPED>(), 3.3},
+      {ECMC_LAYOUT_3, 3, resident_chains<3, 1>(), 3.1},
+      {ECMC_LAYOUT_3C, 3, resident_chains<3, ECMC_CAPPED>(), 3.6},
+  };
+  if (lanes == 1) return ECMC_LAYOUT_1;
+  int best = lanes == 3 ? ECMC_LAYOUT_3C : ECMC_LAYOUT_6;
+  double best_rate = -1.0;
+  for (const Shape& sh : shapes) {
+    if ((lanes != 0 && sh.lanes != lanes) || sh.cap == 0) continue;
+    const double waves = (double)((n_chains + sh.cap - 1) / sh.cap);
+    const double r = sh.rate * (double)n_chains / ((double)sh.cap * (waves < 1.0 ? 1.0 : waves));
+    if (r > best_rate) best_rate = r, best = sh.layout;
+  }
+  return best;
+}
+
+cudaError_t launch_ecmc_sample(const EcmcLaunch& a, int layout, cudaStream_t s) {
+  switch (layout) {
+    case ECMC_LAYOUT_1: return launch_sample<1, 1>(a, s);
+    case ECMC_LAYOUT_3: return launch_sample<3, 1>(a, s);
+    case ECMC_LAYOUT_3C: return launch_sample<3, ECMC_CAPPED>(a, s);
+    case ECMC_LAYOUT_6: return launch_sample<6, 1>(a, s);
+    case ECMC_LAYOUT_6C: return launch_sample<6, ECMC_CAPPED>(a, s);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_ecmc_counters(qcb_ecmc_chain* chains, uint32_t n, unsigned long long* out, int reset,

@@ -170,6 +170,8 @@ SIGNATURES = {
     "qcb_ecmc_create": (C.c_int, [_vp, C.POINTER(EcmcParams), C.c_uint64, C.POINTER(C.c_void_p)]),
     "qcb_ecmc_destroy": (C.c_int, [_vp]),
     "qcb_ecmc_num_chains": (C.c_int, [_vp, _ip]),
+    "qcb_ecmc_set_lanes": (C.c_int, [_vp, C.c_int]),
+    "qcb_ecmc_lanes": (C.c_int, [_vp, _ip]),
     "qcb_ecmc_sample": (C.c_int, [_vp, _ip]),
     "qcb_ecmc_sample_n": (C.c_int, [_vp, _ip, C.c_int]),
     "qcb_ecmc_counters": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.c_int]),

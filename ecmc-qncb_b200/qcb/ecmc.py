@@ -54,6 +54,18 @@ class EventChains:
         self.n_chains = n.value
         field.ctx._adopt(self)
 
+    @property
+    def lanes(self) -> int:
+        """Lanes of a warp per chain in the next call (1, 3 or 6)."""
+        n = C.c_int()
+        check(lib().qcb_ecmc_lanes(self.h, C.byref(n)))
+        return n.value
+
+    @lanes.setter
+    def lanes(self, lanes: int) -> None:
+        """1, 3 or 6 lanes per chain, or 0 to let the library choose; results are the same."""
+        check(lib().qcb_ecmc_set_lanes(self.h, int(lanes)))
+
     def sample(self, shift=(0, 0, 0, 0)) -> None:
         """One sample call of every chain (asynchronous); shift = cumulative shift of the field."""
         check(lib().qcb_ecmc_sample(self.h, (C.c_int * 4)(*[int(s) for s in shift])))

@@ -363,6 +363,12 @@ typedef struct qcb_ecmc_chain {
 int qcb_ecmc_create(qcb_lattice* lat, const qcb_ecmc_params* params, uint64_t seed, qcb_ecmc** out);
 int qcb_ecmc_destroy(qcb_ecmc* e);
 int qcb_ecmc_num_chains(const qcb_ecmc* e, int* n);
+/* Lanes of a warp that run one chain: 1, 3 or 6 (each lane computes an equal share of an
+ * event's six staples, lanes 0-2 also one product each of a lift), or 0 to let the library
+ * choose from the number of chains (the default).  Results do not depend on it, bit for
+ * bit.  qcb_ecmc_lanes returns the lanes the next call will use. */
+int qcb_ecmc_set_lanes(qcb_ecmc* e, int lanes);
+int qcb_ecmc_lanes(const qcb_ecmc* e, int* lanes);
 /* One sample call of every chain (asynchronous).  shift = cumulative shift of the field. */
 int qcb_ecmc_sample(qcb_ecmc* e, const int shift[4]);
 /* n sample calls in a row, call k with the cumulative shift shifts[4k .. 4k+3], with the

@@ -286,3 +286,39 @@ def test_sample_n_equals_single_calls(ctx):
     assert np.array_equal(fa.get_links(), fb.get_links())
     for o in (a, b, fa, fb):
         o.close()
+
+
+@pytest.mark.parametrize("dims,l", [((8, 8, 8, 8), 4), ((12, 12, 12, 12), 3)])
+def test_lanes_per_chain_give_identical_results(ctx, dims, l):
+    """One, three or six lanes per chain (qcb_ecmc_set_lanes) and the automatic choice run
+    the same operations per chain: links and chain records agree bit for bit."""
+    u = orc.hot_philox(dims, 5)
+    shifts = np.array([[1, 0, 2, 1], [2, 1, 0, 0], [0, 2, 1, 1]]) % l
+    out = {}
+    for lanes in (0, 1, 3, 6):
+        f = qcb.GaugeField(ctx, dims)
+        f.set_links(u)
+        ch = qcb.EventChains(f, qcb.ecmc.params(theta_sample=20.0, theta_refresh_site=7.3, theta_refresh_R=3.1,
+                                                l_core=l), 77)
+        ch.lanes = lanes
+        assert ch.lanes == (lanes or ch.lanes) and ch.lanes in (1, 3, 6)
+        for s in shifts:
+            ch.sample(s)
+        rec, _ = ch.chains()
+        assert ch.counters()[0] > 0
+        out[lanes] = (f.get_links(), rec)
+        ch.close()
+        f.close()
+    for lanes in (1, 3, 6):
+        assert np.array_equal(out[lanes][0], out[0][0]), lanes
+        assert np.array_equal(out[lanes][1], out[0][1]), lanes
+
+
+def test_lanes_argument_checked(ctx):
+    f = qcb.GaugeField(ctx, (8, 8, 8, 8))
+    ch = qcb.EventChains(f, BASE, 1)
+    for bad in (-1, 2, 4, 32):
+        with pytest.raises(qcb.QcbError):
+            ch.lanes = bad
+    ch.close()
+    f.close()
