@@ -193,16 +193,20 @@ struct Herm {
   double d[3];  // real diagonal
   Z o[3];       // Q01, Q02, Q12 (Q10 = conj Q01, ...)
 };
-__device__ __forceinline__ Herm ds_matrix(const M& R) {
+// Q from columns 0 and 1 of R (or of the proposal S R).
+__device__ __forceinline__ Herm ds_matrix_cols(const Z c0[3], const Z c1[3]) {
   Herm q;
 #pragma unroll
   for (int m = 0; m < 3; ++m)
-    q.d[m] = R.e[m][0].re * R.e[m][0].re + R.e[m][0].im * R.e[m][0].im - R.e[m][1].re * R.e[m][1].re -
-             R.e[m][1].im * R.e[m][1].im;
-  q.o[0] = R.e[0][0] * conj(R.e[1][0]) - R.e[0][1] * conj(R.e[1][1]);
-  q.o[1] = R.e[0][0] * conj(R.e[2][0]) - R.e[0][1] * conj(R.e[2][1]);
-  q.o[2] = R.e[1][0] * conj(R.e[2][0]) - R.e[1][1] * conj(R.e[2][1]);
+    q.d[m] = fma(c0[m].re, c0[m].re, c0[m].im * c0[m].im) - fma(c1[m].re, c1[m].re, c1[m].im * c1[m].im);
+  q.o[0] = cfma(c0[0], conj(c0[1]), cmul(mk(-c1[0].re, -c1[0].im), conj(c1[1])));
+  q.o[1] = cfma(c0[0], conj(c0[2]), cmul(mk(-c1[0].re, -c1[0].im), conj(c1[2])));
+  q.o[2] = cfma(c0[1], conj(c0[2]), cmul(mk(-c1[1].re, -c1[1].im), conj(c1[2])));
   return q;
+}
+__device__ __forceinline__ Herm ds_matrix(const M& R) {
+  const Z c0[3] = {R.e[0][0], R.e[1][0], R.e[2][0]}, c1[3] = {R.e[0][1], R.e[1][1], R.e[2][1]};
+  return ds_matrix_cols(c0, c1);
 }
 __device__ __forceinline__ int dsign(double x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
 
@@ -251,17 +255,6 @@ __device__ __forceinline__ int lift_link(int i, bool fwd, const int lc[4], int m
   }
 }
 
-// Q = R diag(1, -1, 0) R^dagger from columns 0 and 1 of R.
-__device__ __forceinline__ Herm ds_matrix_cols(const Z c0[3], const Z c1[3]) {
-  Herm q;
-#pragma unroll
-  for (int m = 0; m < 3; ++m)
-    q.d[m] = c0[m].re * c0[m].re + c0[m].im * c0[m].im - c1[m].re * c1[m].re - c1[m].im * c1[m].im;
-  q.o[0] = c0[0] * conj(c0[1]) - c1[0] * conj(c1[1]);
-  q.o[1] = c0[0] * conj(c0[2]) - c1[0] * conj(c1[2]);
-  q.o[2] = c0[1] * conj(c0[2]) - c1[1] * conj(c1[2]);
-  return q;
-}
 
 // The lift's plaquette (lift_improved_fast, ecmc_mpi_cb.cpp:277-337) as F0 F1 F2 F3 with
 // F0 = U0, F2 = U2^+ and, forward, F1 = U1, F3 = U3^+ or, backward, F1 = U1^+, F3 = U3.  The
@@ -689,7 +682,13 @@ __global__ void __launch_bounds__(ECMC_WARPS * 32, MINB) k_ecmc_sample(EcmcLaunc
           const double2 v = sq[cc];
           Sx.e[cc / 3][cc % 3] = mk(v.x, v.y);
         }
-        R = mul_nn(Sx, R);
+        M Rn;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j2 = 0; j2 < 3; ++j2)
+            Rn.e[i][j2] = cdot3(Sx.e[i][0], R.e[0][j2], Sx.e[i][1], R.e[1][j2], Sx.e[i][2], R.e[2][j2]);
+        R = Rn;
         new_eps = -dsign(ds_new);
       }
       const int nmu = lift_link(idx, fwd, lc, mu, nu, t4);
