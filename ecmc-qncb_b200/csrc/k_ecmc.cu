@@ -157,23 +157,26 @@ __device__ __forceinline__ void shifted(const int a[4], int d1, int s1, int d2, 
 // solve_reject_fast (src/ecmc/ecmc_mpi_cb.h:59-94): along U(theta) = R diag(e^{i eps theta},
 // e^{-i eps theta}, 1) R^dagger U one staple's action is A cos(theta) + eps B sin(theta) +
 // const; the angle at which the integral of its derivative's positive part reaches gamma.
+// The reference forms theta = phi + asin(alpha) with phi = atan2(-A, B); here the same angle
+// is one atan2 of (sin, cos)(phi + asin(alpha)), from cos phi = B / R, sin phi = -A / R and
+// cos asin(alpha) = sqrt(1 - alpha^2), and phi's quadrant test (phi < pi/2 or > 3pi/2) is
+// B > 0.  Exact in real arithmetic; the two differ only where B / |A| is below the rounding
+// of phi.
 __device__ double solve_reject(double A, double B, double gamma, int eps) {
   if (eps == -1) B = -B;
   const double R = hypot(A, B), invR = 1.0 / R, period = 2.0 * R;
   const double disc = floor(gamma / period);
   gamma -= disc * period;
-  double phi = atan2(-A, B);
-  if (phi < 0.0) phi += 2.0 * PI;
   const double p1 = R - A;
   double alpha;
-  if (phi < PI * 0.5 || phi > PI * 1.5)
+  if (B > 0.0)
     alpha = (gamma > p1) ? (gamma - p1) * invR - 1.0 : (gamma + A) * invR;
   else
     alpha = gamma * invR - 1.0;
   alpha = alpha > 1.0 ? 1.0 : (alpha < -1.0 ? -1.0 : alpha);
-  double theta = phi + asin(alpha);
+  const double ca = sqrt(fma(-alpha, alpha, 1.0)), sp = -A * invR, cp = B * invR;
+  double theta = atan2(fma(sp, ca, cp * alpha), fma(cp, ca, -(sp * alpha)));
   if (theta < 0.0) theta += 2.0 * PI;
-  if (theta >= 2.0 * PI) theta -= 2.0 * PI;
   return theta + 2.0 * PI * disc;
 }
 
