@@ -322,3 +322,17 @@ def test_lanes_argument_checked(ctx):
             ch.lanes = bad
     ch.close()
     f.close()
+
+
+def test_automatic_lanes_follow_the_chain_count(ctx):
+    """Few chains run on six lanes each; past what the device holds at once, on three."""
+    for dims, l, lanes in (((8, 8, 8, 8), 4, 6), ((30, 30, 30, 30), 3, 3)):
+        f = qcb.GaugeField(ctx, dims, "fp32", 12)
+        ch = qcb.EventChains(f, BASE | {"l_core": l}, 1)
+        assert ch.lanes == lanes, (ch.n_chains, ch.lanes)
+        ch.lanes = 1
+        assert ch.lanes == 1
+        ch.lanes = 0
+        assert ch.lanes == lanes
+        ch.close()
+        f.close()
