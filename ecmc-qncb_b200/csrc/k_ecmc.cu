@@ -160,12 +160,14 @@ __device__ __forceinline__ void shifted(const int a[4], int d1, int s1, int d2, 
 // The reference forms theta = phi + asin(alpha) with phi = atan2(-A, B); here the same angle
 // is one atan2 of (sin, cos)(phi + asin(alpha)), from cos phi = B / R, sin phi = -A / R and
 // cos asin(alpha) = sqrt(1 - alpha^2), and phi's quadrant test (phi < pi/2 or > 3pi/2) is
-// B > 0.  Exact in real arithmetic; the two differ only where B / |A| is below the rounding
+// B > 0; R = hypot(A, B) and 1 / R come from one rsqrt of A^2 + B^2 (A and B are of order
+// beta, far from overflow), and gamma / (2 R) is a product.  Exact in real arithmetic; the
+// forms differ in rounding, and in the branch taken only where B / |A| is below the rounding
 // of phi.
 __device__ double solve_reject(double A, double B, double gamma, int eps) {
   if (eps == -1) B = -B;
-  const double R = hypot(A, B), invR = 1.0 / R, period = 2.0 * R;
-  const double disc = floor(gamma / period);
+  const double R2 = fma(A, A, B * B), invR = rsqrt(R2), R = R2 * invR, period = 2.0 * R;
+  const double disc = floor(gamma * (0.5 * invR));
   gamma -= disc * period;
   const double p1 = R - A;
   double alpha;
