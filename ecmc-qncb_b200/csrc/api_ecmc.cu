@@ -229,7 +229,7 @@ int qcb_ecmc_set_chains(qcb_ecmc* e, const qcb_ecmc_chain* chains, uint64_t call
   for (uint32_t i = 0; i < e->n_chains; ++i) {
     const qcb_ecmc_chain& r = chains[i];
     if (!r.initialized) continue;
-    bool ok = r.mu >= 0 && r.mu < 4 && (r.epsilon >= -1 && r.epsilon <= 1);
+    bool ok = r.mu >= 0 && r.mu < 4 && (r.epsilon == -1 || r.epsilon == 1);
     for (int d = 0; d < 4; ++d) ok = ok && r.site[d] >= -(1 << 20) && r.site[d] <= (1 << 20);
     if (!ok) return efail(QCB_ERR_INVALID, "chain " + std::to_string(i) + " has a direction, sense or site out of range");
   }

@@ -167,10 +167,13 @@ def test_argument_checks(ctx):
     ch = qcb.EventChains(f, BASE, 1)
     rec = np.zeros(ch.n_chains, CHAIN_DTYPE)
     rec["initialized"] = 1
-    rec["mu"] = 4
-    with pytest.raises(qcb.QcbError) as e:
-        ch.set_chains(rec, 0)
-    assert e.value.code == 1
+    rec["epsilon"] = 1
+    for field, value in (("mu", 4), ("mu", -1), ("epsilon", 0), ("epsilon", 2)):
+        bad = rec.copy()
+        bad[field] = value
+        with pytest.raises(qcb.QcbError) as e:
+            ch.set_chains(bad, 0)
+        assert e.value.code == 1
     ch.close()
     f.close()
 
