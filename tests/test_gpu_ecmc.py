@@ -291,8 +291,9 @@ def test_sample_n_equals_single_calls(ctx):
         o.close()
 
 
-@pytest.mark.parametrize("dims,l", [((8, 8, 8, 8), 4), ((12, 12, 12, 12), 3)])
-def test_lanes_per_chain_give_identical_results(ctx, dims, l):
+@pytest.mark.parametrize("dims,l,poisson,eps_set", [((8, 8, 8, 8), 4, False, 0.15), ((12, 12, 12, 12), 3, False, 0.15),
+                                                     ((8, 8, 8, 8), 4, True, 0.15), ((10, 10, 10, 10), 5, True, 0.3)])
+def test_lanes_per_chain_give_identical_results(ctx, dims, l, poisson, eps_set):
     """One, three or six lanes per chain (qcb_ecmc_set_lanes) and the automatic choice run
     the same operations per chain: links and chain records agree bit for bit."""
     u = orc.hot_philox(dims, 5)
@@ -302,7 +303,7 @@ def test_lanes_per_chain_give_identical_results(ctx, dims, l):
         f = qcb.GaugeField(ctx, dims)
         f.set_links(u)
         ch = qcb.EventChains(f, qcb.ecmc.params(theta_sample=20.0, theta_refresh_site=7.3, theta_refresh_R=3.1,
-                                                l_core=l), 77)
+                                                poisson=poisson, epsilon_set=eps_set, l_core=l), 77)
         ch.lanes = lanes
         assert ch.lanes == (lanes or ch.lanes) and ch.lanes in (1, 3, 6)
         for s in shifts:
