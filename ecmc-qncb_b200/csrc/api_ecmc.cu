@@ -135,6 +135,9 @@ int qcb_ecmc_set_lanes(qcb_ecmc* e, int lanes) {
 
 int qcb_ecmc_lanes(const qcb_ecmc* e, int* lanes) {
   if (!e || !lanes) return efail(QCB_ERR_INVALID, "null argument");
+  qcb_ctx* c = e->ctx;
+  std::lock_guard<std::mutex> lk(c->mu);
+  ECU(cudaSetDevice(c->device), "cudaSetDevice");
   const int layout = ecmc_layout(e->n_chains, e->lanes);
   *lanes = layout == ECMC_LAYOUT_1 ? 1 : (layout == ECMC_LAYOUT_6 || layout == ECMC_LAYOUT_6C ? 6 : 3);
   return QCB_OK;
@@ -169,16 +172,32 @@ int qcb_ecmc_sample_n(qcb_ecmc* e, const int* shifts, int n) {
   ECU(launch_soa_to_aos(L->dev, reinterpret_cast<double*>(e->d_links), 0, L->dev.g.V, 0, c->stream, 0),
       "links to FP64 array-of-structures");
   c->launches++;
-  for (int k = 0; k < n; ++k) {
+  // A launch that fails part-way leaves the calls before it complete: their link updates are
+  // still unpacked into the lattice below, so the lattice and the chain records (and the call
+  // count) stay consistent, and the failure is returned after the unpack.
+  cudaError_t err = cudaSuccess;
+  const char* what = nullptr;
+  const int layout = ecmc_layout(e->n_chains, e->lanes);
+  for (int k = 0; k < n && err == cudaSuccess; ++k) {
     for (int d = 0; d < 4; ++d) a.cum[d] = ((shifts[4 * k + d] % a.L[d]) + a.L[d]) % a.L[d];
-    ECU(launch_ecmc_set(e->d_set, e->p.epsilon_set, e->seed, e->calls, c->stream), "ECMC set");
-    ECU(launch_ecmc_sample(a, ecmc_layout(e->n_chains, e->lanes), c->stream), "ECMC sample");
-    c->launches += 2;
+    err = launch_ecmc_set(e->d_set, e->p.epsilon_set, e->seed, e->calls, c->stream);
+    if (err != cudaSuccess) {
+      what = "ECMC set";
+      break;
+    }
+    c->launches++;
+    err = launch_ecmc_sample(a, layout, c->stream);
+    if (err != cudaSuccess) {
+      what = "ECMC sample";
+      break;
+    }
+    c->launches++;
     e->calls++;
   }
   ECU(launch_aos_to_soa(L->dev, reinterpret_cast<const double*>(e->d_links), 0, L->dev.g.V, 0, c->stream, 0),
       "links from FP64 array-of-structures");
   c->launches++;
+  if (err != cudaSuccess) return efail(QCB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
   return QCB_OK;
 }
 

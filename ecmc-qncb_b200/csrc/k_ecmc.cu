@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "ecmc.h"
 #include "philox.cuh"
 #include "su3.cuh"
@@ -787,20 +789,37 @@ uint32_t resident_chains() {
 // similar number of events, so shape k is expected to run at rate_k n / (cap_k ceil(n / cap_k)),
 // rate_k being its event rate with the device full.  The rates are the ones measured on B200
 // (1e8 events/s, reference default budgets, 8192 to 65536 chains); the capacities come from
-// the occupancy calculator.  Among equal estimates the earlier shape wins.
+// the occupancy calculator.  Among equal estimates the earlier shape wins.  The capacities are
+// computed once per device, for the device current at the call (callers make the lattice's
+// device current first).
 int ecmc_layout(uint32_t n_chains, int lanes) {
   struct Shape {
     int layout, lanes;
     uint32_t cap;
     double rate;
   };
-  static const Shape shapes[] = {
-      {ECMC_LAYOUT_6, 6, resident_chains<6, 1>(), 2.9},
-      {ECMC_LAYOUT_6C, 6, resident_chains<6, ECMC_CAPPED>(), 3.3},
-      {ECMC_LAYOUT_3, 3, resident_chains<3, 1>(), 3.1},
-      {ECMC_LAYOUT_3C, 3, resident_chains<3, ECMC_CAPPED>(), 3.6},
-  };
+  constexpr int MAX_DEVICES = 64;
+  static std::mutex mu;
+  static bool filled[MAX_DEVICES] = {};
+  static Shape table[MAX_DEVICES][4];
   if (lanes == 1) return ECMC_LAYOUT_1;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) dev = 0;
+  Shape shapes[4];
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!filled[dev]) {
+      const Shape t[4] = {
+          {ECMC_LAYOUT_6, 6, resident_chains<6, 1>(), 2.9},
+          {ECMC_LAYOUT_6C, 6, resident_chains<6, ECMC_CAPPED>(), 3.3},
+          {ECMC_LAYOUT_3, 3, resident_chains<3, 1>(), 3.1},
+          {ECMC_LAYOUT_3C, 3, resident_chains<3, ECMC_CAPPED>(), 3.6},
+      };
+      for (int k = 0; k < 4; ++k) table[dev][k] = t[k];
+      filled[dev] = true;
+    }
+    for (int k = 0; k < 4; ++k) shapes[k] = table[dev][k];
+  }
   int best = lanes == 3 ? ECMC_LAYOUT_3C : ECMC_LAYOUT_6;
   double best_rate = -1.0;
   for (const Shape& sh : shapes) {

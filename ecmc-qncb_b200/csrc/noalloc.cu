@@ -12,11 +12,14 @@
 // the library holds until the process exits.
 //
 // The array's name in host code is only a host-side stand-in for the symbol, not a device
-// address, so its device address is looked up once per device with cudaGetSymbolAddress
-// (with that device current) on the first call there, and passed to the kernels.  Every
+// address, so every call looks up its device address with cudaGetSymbolAddress (with the
+// caller's device current; the lookup allocates nothing) and passes that to the kernels.
+// Looking it up on every call, rather than caching it per device, keeps the address right
+// when the host application resets the device and the module is loaded again.  The first
+// call on a device loads the module, so it should come before any stream capture.  Every
 // call shares the array; calls whose kernels overlap on the GPU race on it.  Nothing in it
 // needs to start at zero: each launch writes every partial it later reads.
-#include <mutex>
+#include <stdint.h>
 
 #include "../../include/qcb.h"
 #include "kernels.h"
@@ -24,10 +27,6 @@
 namespace {
 
 static __device__ __align__(256) double g_noalloc_scratch[QCB_NOALLOC_MAX_PARTIALS];
-
-constexpr int MAX_DEVICES = 64;
-std::mutex g_mu;
-double* g_scratch_addr[MAX_DEVICES] = {};
 
 __global__ void k_mean(double* out, double inv_count) { out[0] *= inv_count; }
 
@@ -37,6 +36,12 @@ extern "C" int qcb_plaquette_noalloc(const void* links, const int dims[4], int p
                                      double* out, void* stream) {
   using namespace qcb;
   if (!links || !dims || !out) return set_error(QCB_ERR_INVALID, "null argument");
+  // The kernels read a link chunk as one 16-byte vector (8 bytes for FP32 18-real storage)
+  // and write one double: a sub-allocated pointer off those boundaries would fault the device.
+  const uintptr_t chunk = (precision == QCB_FP32 && storage == QCB_R18) ? 8 : 16;
+  if ((uintptr_t)links % chunk)
+    return set_error(QCB_ERR_INVALID, "links must be aligned to the storage's chunk size (16 bytes; 8 for FP32 18-real)");
+  if ((uintptr_t)out % alignof(double)) return set_error(QCB_ERR_INVALID, "out must be 8-byte aligned");
   uint64_t vol = 1;
   for (int d = 0; d < 4; ++d) {
     if (dims[d] < 2 || (dims[d] & 1)) return set_error(QCB_ERR_INVALID, "lattice extents must be even and >= 2");
@@ -60,21 +65,9 @@ extern "C" int qcb_plaquette_noalloc(const void* links, const int dims[4], int p
   if (nblocks > QCB_NOALLOC_MAX_PARTIALS)
     return set_error(QCB_ERR_INVALID, "reduction needs more partial sums than the static scratch holds");
 
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return set_error(QCB_ERR_CUDA, cudaGetErrorString(e));
-  if (dev < 0 || dev >= MAX_DEVICES) return set_error(QCB_ERR_INVALID, "device index above the supported range");
   double* scratch = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_addr[dev]) {
-      double* p = nullptr;
-      e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
-      if (e != cudaSuccess) return set_error(QCB_ERR_CUDA, cudaGetErrorString(e));
-      g_scratch_addr[dev] = p;
-    }
-    scratch = g_scratch_addr[dev];
-  }
+  cudaError_t e = cudaGetSymbolAddress((void**)&scratch, g_noalloc_scratch);
+  if (e != cudaSuccess) return set_error(QCB_ERR_CUDA, cudaGetErrorString(e));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   e = launch_plaquette_partials(L, nblocks, scratch, out, s);
   if (e == cudaSuccess) {

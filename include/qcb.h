@@ -155,10 +155,13 @@ int qcb_topo_qe(qcb_lattice* lat, double* q, double* e);
  * qcb_lattice_device_links), written to out[0] (caller-owned device memory) on `stream`
  * (a cudaStream_t; NULL = legacy default stream), asynchronously.  It calls no cudaMalloc,
  * cudaFree or other allocating routine: its reduction scratch is a static device array of
- * QCB_NOALLOC_MAX_PARTIALS doubles (16 KiB per GPU, held until the process exits).  The
- * first call on a device looks up that array's device address (make it before any stream
- * capture).  Calls share the array, so calls that overlap on the GPU race; requests that
- * would need more partial sums than the array holds are rejected with QCB_ERR_INVALID. */
+ * QCB_NOALLOC_MAX_PARTIALS doubles (16 KiB per GPU, held until the process exits).  Every
+ * call looks up that array's device address for the current device; the first call on a
+ * device also loads the library's device code there (make it before any stream capture).
+ * Calls share the array, so calls that overlap on the GPU race; requests that would need
+ * more partial sums than the array holds are rejected with QCB_ERR_INVALID, and so are
+ * links not aligned to the storage's chunk size (16 bytes; 8 for FP32 18-real) and an out
+ * pointer not aligned to 8 bytes. */
 #define QCB_NOALLOC_MAX_PARTIALS 2048
 int qcb_plaquette_noalloc(const void* links, const int dims[4], int precision, int storage, size_t stride,
                           double* out, void* stream);
@@ -373,7 +376,9 @@ int qcb_ecmc_lanes(const qcb_ecmc* e, int* lanes);
 int qcb_ecmc_sample(qcb_ecmc* e, const int shift[4]);
 /* n sample calls in a row, call k with the cumulative shift shifts[4k .. 4k+3], with the
  * lattice packed into the chains' FP64 copy once before and unpacked once after: the same
- * result as n qcb_ecmc_sample calls, bit for bit (asynchronous). */
+ * result as n qcb_ecmc_sample calls, bit for bit (asynchronous).  If a launch fails after
+ * k calls, those k calls stay complete: their link updates are unpacked into the lattice,
+ * the chain records and the call count cover exactly them, and QCB_ERR_CUDA is returned. */
 int qcb_ecmc_sample_n(qcb_ecmc* e, const int* shifts, int n);
 /* Waits, then sums the chains' events, lifts and same-site lifts into out[0..2]; with reset,
  * zeroes the three counters afterwards (the reference resets them after each plaquette

@@ -48,6 +48,16 @@ def test_null_arguments_are_rejected():
     assert L.qcb_ecmc_num_chains(None, None) == 1
 
 
+def test_noalloc_plaquette_rejects_misaligned_pointers_before_any_launch():
+    L = _lib.lib()
+    dims = (C.c_int * 4)(8, 8, 8, 8)
+    for prec, nr, ptr in ((0, 18, 24), (1, 12, 40), (1, 18, 20)):
+        assert L.qcb_plaquette_noalloc(C.c_void_p(ptr), dims, prec, nr, 2048, C.c_void_p(16), None) == 1
+        assert b"aligned" in L.qcb_last_error()
+    assert L.qcb_plaquette_noalloc(C.c_void_p(16), dims, 0, 18, 2048, C.c_void_p(4), None) == 1
+    assert b"out must be 8-byte aligned" in L.qcb_last_error()
+
+
 def test_context_creation_without_gpu_fails_cleanly():
     if qcb.device_count() > 0:
         pytest.skip("a CUDA device is present")

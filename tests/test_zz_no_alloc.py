@@ -50,6 +50,36 @@ def test_plaquette_noalloc_matches_allocating_entry_point():
     ctx.close()
 
 
+def test_plaquette_noalloc_allocates_nothing_and_runs_on_any_stream():
+    """After a warm-up call, further calls leave the device's free memory unchanged, and a
+    call on a stream other than the context's gives the same value."""
+    import torch
+
+    ctx = qcb.Context(0)
+    f = qcb.GaugeField(ctx, (8, 8, 8, 8), "fp32", 12)
+    f.hot_start(3)
+    ref = qcb.observables.mean_plaquette_global(f)
+    out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
+    side = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    noalloc_plaquette(f, out.data_ptr(), ctx.stream)  # warm-up: loads the module's device code
+    ctx.sync()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        noalloc_plaquette(f, out.data_ptr(), ctx.stream)
+    ctx.sync()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    out.fill_(float("nan"))
+    torch.cuda.synchronize()
+    noalloc_plaquette(f, out.data_ptr() + 8, side.cuda_stream)
+    side.synchronize()
+    got = float(out[1].item())
+    assert abs(got - ref) <= TOL * abs(ref), (got, ref)
+    f.close()
+    ctx.close()
+
+
 def test_plaquette_noalloc_rejects_bad_arguments():
     L = _lib.lib()
     dims = (C.c_int * 4)(8, 8, 8, 8)
@@ -62,3 +92,11 @@ def test_plaquette_noalloc_rejects_bad_arguments():
     # stride below half the volume
     assert L.qcb_plaquette_noalloc(C.c_void_p(16), dims, 0, 18, 100, C.c_void_p(16), None) == 1
     assert b"stride" in L.qcb_last_error()
+    # links off the 16-byte chunk boundary (FP64, FP32 12-real) or the 8-byte one (FP32 18-real)
+    assert L.qcb_plaquette_noalloc(C.c_void_p(24), dims, 0, 18, 2048, C.c_void_p(16), None) == 1
+    assert b"aligned" in L.qcb_last_error()
+    assert L.qcb_plaquette_noalloc(C.c_void_p(24), dims, 1, 12, 2048, C.c_void_p(16), None) == 1
+    assert L.qcb_plaquette_noalloc(C.c_void_p(20), dims, 1, 18, 2048, C.c_void_p(16), None) == 1
+    # output not 8-byte aligned
+    assert L.qcb_plaquette_noalloc(C.c_void_p(16), dims, 0, 18, 2048, C.c_void_p(12), None) == 1
+    assert b"out must be 8-byte aligned" in L.qcb_last_error()
