@@ -428,6 +428,7 @@ def _ecmc_cpu_worker(args):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
 
+    oracle.select_build("fast")
     p = dict(beta=BETA, theta_sample=ECMC_THETA, theta_refresh_site=50.0, theta_refresh_R=15.0, epsilon_set=0.15,
              poisson=0)
     run = oracle.EcmcRefRun(ECMC_LCORE, seed, False, p)
@@ -443,6 +444,10 @@ def _ecmc_cpu_worker(args):
 def ecmc_cpu_reference(budget_s: float = 8.0) -> dict:
     """The reference's event-chain algorithm with its own generator on the host cores, one
     process per core as one rank each (see _ecmc_cpu_worker)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    oracle.build_fast()
     cores = min(64, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1))
     with mp.get_context("spawn").Pool(cores) as pool:
         res = pool.map(_ecmc_cpu_worker, [(500 + r, budget_s) for r in range(cores)])
@@ -450,7 +455,7 @@ def ecmc_cpu_reference(budget_s: float = 8.0) -> dict:
             "kind": "port",
             "sample": f"{cores} processes, each one rank of the reference (one chain on a {ECMC_LCORE}^4 block, the "
                       f"reference's std::mt19937_64 generator and per-call set), theta_sample {ECMC_THETA:g} calls "
-                      f"for {budget_s:g} s"}
+                      f"for {budget_s:g} s; oracle built -O3 -march=native -fcx-limited-range"}
 
 
 def ecmc_section(ctx, steps=5, warmup=3, cpu_budget_s=8.0, cpu=True):
@@ -730,6 +735,7 @@ def _plain_cpu(_):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
 
+    oracle.select_build("fast")
     t = time.perf_counter()
     chain = oracle.RefChain(8, 1234, True)
     chain.run(6.0, 200, 1, 1)
@@ -763,6 +769,10 @@ def plain_section():
         t_flow = time.perf_counter() - t
         f.close()
         ctx.close()
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    oracle.build_fast()
     with mp.get_context("spawn").Pool(1) as pool:
         t_cpu = pool.map(_plain_cpu, [0])[0]
     return {"workload": "8^4 beta=6.0 cold start seed 1234, 200 sweeps + plaquette each; flow eps=0.02, 50 steps",
@@ -778,6 +788,7 @@ def _ref_worker(args):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
 
+    oracle.select_build("fast")
     chain = oracle.RefChain(lb, seed, False)
     t = time.perf_counter()
     chain.run(BETA, sweeps, 1, 1)  # shift + sweep + plaquette per shift
@@ -793,11 +804,14 @@ def _ref_worker(args):
 def cpu_baseline(sweeps: int = 1, rk3: int = 1, block: int = 16):
     """Reference algorithm on the host cores: one process per hardware thread (the reference
     runs one MPI rank per core), each on a 16^4 block as in the reference's 2^4-rank
-    decomposition of 32^4; the rates are summed over the processes."""
+    decomposition of 32^4; the rates are summed over the processes.  The oracle runs as its
+    timing build: -O3 for the host's instruction set (the reference's release flags,
+    CMakeLists.txt:88-102), complex products without __muldc3, and a neighbour table as the
+    reference keeps one (GeometryCB.cpp:10-31)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
 
-    oracle.build()
+    oracle.build_fast()
     cores = min(64, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1))
     with mp.get_context("spawn").Pool(cores) as pool:
         t = time.perf_counter()
@@ -808,7 +822,8 @@ def cpu_baseline(sweeps: int = 1, rk3: int = 1, block: int = 16):
     return {"value": hb_rate, "unit": "link-updates/s", "cores": cores, "kind": "port",
             "flow_value": flow_rate, "flow_unit": "site-steps/s", "wall_s": wall,
             "sample": f"{cores} processes x ({sweeps} reference shift+sweep on a {block}^4 block with frozen "
-                      f"links, then {rk3} RK3 flow step); link-updates counted as 4L(L-1)^3 per sweep"}
+                      f"links, then {rk3} RK3 flow step); link-updates counted as 4L(L-1)^3 per sweep; "
+                      f"oracle built -O3 -march=native -fcx-limited-range with a neighbour table"}
 
 
 def main():

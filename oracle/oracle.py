@@ -20,20 +20,74 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_build" / "liborc.so"
 
 _lib = None
+_build_kind = "checker"
 
 
 def build() -> Path:
-    """Compile liborc.so with the committed Makefile (g++, FP64, -O2)."""
+    """Compile liborc.so, the checker, with the committed Makefile (g++, FP64, -O2, no FMA
+    contraction on the baseline x86-64 target, so its rounding is fixed)."""
     subprocess.run(["make", "-s", "-f", str(HERE / "Makefile")], check=True)
     return LIB_PATH
+
+
+def _host_tag() -> str:
+    """Short hash of the host CPU's model and feature flags: the timing build targets the
+    host it runs on (-march=native), so each kind of host gets its own file."""
+    import hashlib
+
+    info = ""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith(("model name", "flags")):
+                info += line
+                if line.startswith("flags"):
+                    break
+    except OSError:
+        pass
+    return hashlib.sha1(info.encode()).hexdigest()[:12]
+
+
+def fast_lib_path() -> Path:
+    return HERE / "_build" / f"liborc_fast-{_host_tag()}.so"
+
+
+def build_fast() -> Path:
+    """Compile the timing build of the same source as the reference's release build is
+    compiled (CMakeLists.txt:88-102: -O3 with the host's instruction set): -O3 -march=native
+    -fcx-limited-range (complex products without the __muldc3 call).  Only the CPU baseline
+    uses it; its rounding differs from the checker's (FMA contraction)."""
+    out = fast_lib_path()
+    subprocess.run(["make", "-s", "-f", str(HERE / "Makefile"), "fast", f"FAST_OUT={out}"], check=True)
+    return out
+
+
+def select_build(kind: str) -> None:
+    """'checker' (default): liborc.so.  'fast': the timing build for this host, built on
+    first use.  Must be called before the first call into the oracle in this process."""
+    global _build_kind
+    if _lib is not None and kind != _build_kind:
+        raise RuntimeError("the oracle library is already loaded")
+    if kind not in ("checker", "fast"):
+        raise ValueError(kind)
+    _build_kind = kind
+
+
+def build_flags() -> str:
+    return "-O2 (checker)" if _build_kind == "checker" else "-O3 -march=native -fcx-limited-range, neighbour table"
 
 
 def lib():
     global _lib
     if _lib is None:
-        if not LIB_PATH.exists():
-            build()
-        L = C.CDLL(str(LIB_PATH))
+        if _build_kind == "fast":
+            path = fast_lib_path()
+            if not path.exists():
+                build_fast()
+        else:
+            path = LIB_PATH
+            if not path.exists():
+                build()
+        L = C.CDLL(str(path))
         dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
         u32p = C.POINTER(C.c_uint32)
         L.orc_plaquette.argtypes = [dp, ip, dp]

@@ -90,6 +90,10 @@ struct Lat {
   int L[4];
   size_t V;
   C* u;  // borrowed, 36*V complex
+  // Optional neighbour table (borrowed): nbt[8 s + 2 mu + 0] = s + mu, [.. + 1] = s - mu.  The
+  // reference keeps such a table (src/geometry/GeometryCB.cpp:10-31); it only replaces the
+  // division-based lookup below, so results are the same bit for bit with or without it.
+  const uint32_t* nbt = nullptr;
   size_t idx(int x, int y, int z, int t) const {
     return (size_t)x + (size_t)L[0] * ((size_t)y + (size_t)L[1] * ((size_t)z + (size_t)L[2] * (size_t)t));
   }
@@ -103,6 +107,7 @@ struct Lat {
   }
   // neighbour of s displaced by d (+1 / -1) in direction mu (periodic)
   size_t nb(size_t s, int mu, int d) const {
+    if (nbt) return nbt[8 * s + 2 * mu + (d > 0 ? 0 : 1)];
     int c[4];
     coords(s, c);
     c[mu] = (c[mu] + d + L[mu]) % L[mu];
@@ -122,6 +127,17 @@ static Lat make(double* aos, const int dims[4]) {
   l.V = (size_t)dims[0] * dims[1] * dims[2] * dims[3];
   l.u = reinterpret_cast<C*>(aos);
   return l;
+}
+
+// Fills the neighbour table of lattice f (8 entries per site) and attaches it to f.
+static void attach_nb_table(Lat& f, std::vector<uint32_t>& tab) {
+  tab.resize(8 * f.V);
+  for (size_t s = 0; s < f.V; ++s)
+    for (int mu = 0; mu < 4; ++mu) {
+      tab[8 * s + 2 * mu] = (uint32_t)f.nb(s, mu, +1);
+      tab[8 * s + 2 * mu + 1] = (uint32_t)f.nb(s, mu, -1);
+    }
+  f.nbt = tab.data();
 }
 
 // GaugeField::compute_staple (src/gauge/GaugeField.cpp:74-97)
@@ -562,11 +578,14 @@ struct RefChain {
   std::vector<C> links;
   std::mt19937_64 rng;
   std::vector<C> tmp;
+  std::vector<uint32_t> nbtab;
   Lat lat() {
     Lat l;
     for (int d = 0; d < 4; ++d) l.L[d] = dims[d];
     l.V = (size_t)dims[0] * dims[1] * dims[2] * dims[3];
     l.u = links.data();
+    if (nbtab.empty()) attach_nb_table(l, nbtab);
+    l.nbt = nbtab.data();
     return l;
   }
 };
@@ -1039,6 +1058,8 @@ int orc_flow_measure(const double* aos, const int dims[4], double eps, int n_ste
   size_t V = (size_t)dims[0] * dims[1] * dims[2] * dims[3];
   std::vector<double> copy(aos, aos + V * 72);
   Lat f = make(copy.data(), dims);
+  std::vector<uint32_t> tab;
+  attach_nb_table(f, tab);
   Flow gf{&f, eps, {}, {}};
   double t = 0.0;
   for (int st = 0; st < n_steps_gf; st++) {
@@ -1057,6 +1078,8 @@ int orc_flow_measure(const double* aos, const int dims[4], double eps, int n_ste
 
 int orc_flow_steps(double* aos, const int dims[4], double eps, int n) {
   Lat f = make(aos, dims);
+  std::vector<uint32_t> tab;
+  attach_nb_table(f, tab);
   Flow gf{&f, eps, {}, {}};
   for (int r = 0; r < n; ++r) gf.rk3_step();
   return 0;

@@ -1,4 +1,6 @@
-"""Binned mean / error of a Markov-chain time series (test helper)."""
+"""Binned mean / error of Markov-chain time series (test helper)."""
+import math
+
 import numpy as np
 
 
@@ -31,3 +33,33 @@ def z_score(a, b, nbins: int = 20) -> float:
     ma, ea = binned_mean_err(a, nbins)
     mb, eb = binned_mean_err(b, nbins)
     return abs(ma - mb) / np.hypot(ea, eb)
+
+
+def bin_length(taus, factor: float = 10.0) -> int:
+    """Bin length of at least `factor` times the largest integrated autocorrelation time."""
+    return int(math.ceil(factor * max(taus)))
+
+
+def chain_bins(x, length: int) -> np.ndarray:
+    """Means of consecutive bins of `length` samples (a trailing partial bin is dropped)."""
+    x = np.asarray(x, float)
+    n = (x.size // length) * length
+    return x[:n].reshape(-1, length).mean(axis=1)
+
+
+def pooled_mean_err(bins_per_chain):
+    """Mean and standard error from the bin means of several independent chains, pooled:
+    with bins much longer than the autocorrelation time every bin mean is an independent
+    sample of the same distribution."""
+    b = np.concatenate([np.asarray(c, float) for c in bins_per_chain])
+    return float(b.mean()), float(b.std(ddof=1) / np.sqrt(b.size)), int(b.size)
+
+
+def chains_summary(series, factor: float = 10.0, length: int = 0) -> dict:
+    """tau_int of each chain, the common bin length (>= factor * the largest tau_int, or
+    `length` if that is longer), the bin means of each chain, and the pooled mean and error."""
+    taus = [tau_int(x) for x in series]
+    length = max(length, bin_length(taus, factor))
+    bins = [chain_bins(x, length) for x in series]
+    mean, err, nb = pooled_mean_err(bins)
+    return {"tau_int": taus, "bin_length": length, "bins": bins, "mean": mean, "err": err, "n_bins": nb}
