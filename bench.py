@@ -21,6 +21,7 @@ core on 16^4 blocks as the reference's 2^4-rank decomposition of 32^4 would run.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import multiprocessing as mp
 import os
@@ -269,8 +270,10 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
     plaq_box, tqe_box = [], []
 
     def hb_body():
-        _lib.check(lib.qcb_heatbath(f32.h, BETA, SWEEPS, 1, seed, 0))
-        plaq_box.append(qcb.observables.mean_plaquette_global(f32))
+        # 500 sweeps with the final plaquette summed inside the last sweep (one call)
+        out = ctypes.c_double()
+        _lib.check(lib.qcb_heatbath_plaquette(f32.h, BETA, SWEEPS, 1, seed, 0, ctypes.byref(out)))
+        plaq_box.append(out.value)
 
     e2e_hb_ms = e2e(hb_body)
     e2e_fl_ms = e2e(lambda: tqe_box.append(qcb.observables.topo_charge_flowed(f32, gf, FLOW_RECORDS, FLOW_RK)))
@@ -318,10 +321,25 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
         # The 20 req/s stream offers about three times the work the GPU completes per second,
         # so its latency is set by the queue.  The same job mix at 80% of the measured job
         # throughput shows the latency of a server that keeps up.
-        rate = 0.8 * result["serving"]["throughput_jobs_per_s"]
-        result["serving_80pct_load"] = serving_section(ctx, n_requests=40, rate=rate)
+        cap = result["serving"]["throughput_jobs_per_s"]
+        result["serving_80pct_load"] = serving_section(ctx, n_requests=40, rate=0.8 * cap)
+        # p50 / p99 against the offered rate, below and above the measured job capacity
+        curve = []
+        for frac in (0.5, 1.2, 2.0):
+            r = serving_section(ctx, n_requests=40, rate=frac * cap)
+            curve.append({"offered_req_per_s": frac * cap, "offered_over_capacity": frac, "p50_s": r["p50_s"],
+                          "p99_s": r["p99_s"], "throughput_jobs_per_s": r["throughput_jobs_per_s"]})
+        s80 = result["serving_80pct_load"]
+        curve.append({"offered_req_per_s": 0.8 * cap, "offered_over_capacity": 0.8, "p50_s": s80["p50_s"],
+                      "p99_s": s80["p99_s"], "throughput_jobs_per_s": s80["throughput_jobs_per_s"]})
+        curve.append({"offered_req_per_s": 20.0, "offered_over_capacity": 20.0 / cap,
+                      "p50_s": result["serving"]["p50_s"], "p99_s": result["serving"]["p99_s"],
+                      "throughput_jobs_per_s": cap})
+        result["serving_curve"] = {"capacity_jobs_per_s": cap, "requests_per_point": 40,
+                                   "points": sorted(curve, key=lambda c: c["offered_req_per_s"])}
         result["plain"] = plain_section()
         result["ecmc"] = ecmc_section(ctx, cpu=not args.no_cpu_baseline)
+        result["large"] = large_workload()
     return result
 
 

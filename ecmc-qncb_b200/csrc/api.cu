@@ -360,6 +360,7 @@ int qcb_lattice_destroy(qcb_lattice* L) {
     cudaFree(L->fw[0]);
     cudaFree(L->fw[1]);
     cudaFree(L->fz);
+    cudaFree(L->meas);
     cudaGetLastError();
   }
   delete L;
@@ -671,6 +672,60 @@ int qcb_heatbath(qcb_lattice* L, double beta, int n_sweeps, int n_hits, uint64_t
   return QCB_OK;
 }
 
+int qcb_heatbath_plaquette(qcb_lattice* L, double beta, int n_sweeps, int n_hits, uint64_t seed,
+                           uint64_t sweep_offset, double* plaq) {
+  CHECK_LAT(L);
+  if (L->slab_tl) return fail(QCB_ERR_STATE, "not available on a slab (needs halo exchanges between its passes)");
+  if (!plaq) return fail(QCB_ERR_INVALID, "null output");
+  if (n_sweeps < 0 || n_hits < 0) return fail(QCB_ERR_INVALID, "negative sweep or hit count");
+  if (!(beta > 0.0)) return fail(QCB_ERR_INVALID, "beta must be positive");
+  if (n_hits > (1 << 20)) return fail(QCB_ERR_INVALID, "too many hits");
+  qcb_ctx* c = L->ctx;
+  LOCK(c);
+  TRY(set_device(c));
+  if (n_sweeps == 0) {
+    CU(launch_plaquette(L->dev, c->d_scratch, c->d_out, c->stream, c->block), "plaquette");
+    c->launches += 2;
+  } else {
+    const int nb = hb_meas_blocks(L->dev);
+    const size_t need = 2 * (size_t)nb + 256;
+    if (L->meas_n < need) {
+      cudaFree(L->meas);
+      L->meas = nullptr;
+      L->meas_n = 0;
+      if (cudaMalloc(&L->meas, need * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(QCB_ERR_NOMEM, "cannot allocate the measurement partial sums");
+      }
+      L->meas_n = need;
+    }
+    for (int s = 0; s < n_sweeps; ++s) {
+      const uint32_t sweep = (uint32_t)(sweep_offset + (uint64_t)s);
+      const bool last = s == n_sweeps - 1;
+      for (int mu = 0; mu < 4; ++mu)
+        for (int par = 0; par < 2; ++par) {
+          if (last && mu == 3) {
+            CU(launch_hb_pass_meas(L->dev, par, beta, seed, sweep, n_hits, c->d_status, L->meas + (size_t)par * nb,
+                                   c->stream),
+               "measuring heatbath pass");
+          } else {
+            CU(launch_hb_pass(L->dev, mu, par, beta, seed, sweep, n_hits, c->d_status, c->stream, c->block),
+               "heatbath pass");
+          }
+          c->launches++;
+        }
+    }
+    CU(launch_sum_parts(L->meas, 2 * nb, L->meas + 2 * nb, c->d_out, c->stream), "plaquette sum");
+    c->launches += 2;
+  }
+  CU(cudaMemcpyAsync(c->h_out, c->d_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H");
+  TRY(check_status(c));
+  // the measuring passes sum Re tr P; the plaquette kernel sums Re tr P / 3
+  const double scale = n_sweeps == 0 ? 1.0 : 1.0 / 3.0;
+  *plaq = c->h_out[0] * scale / (6.0 * (double)L->dev.g.Vg);
+  return QCB_OK;
+}
+
 int qcb_heatbath_frozen(qcb_lattice* L, double beta, int n_sweeps, int n_hits, uint64_t seed, uint64_t sweep_offset,
                         int l_core, const int shift[4]) {
   CHECK_LAT(L);
@@ -920,6 +975,34 @@ int qcb_slab_face_copy(qcb_lattice* L, int which, int side, int mu, int parity, 
       CU(cudaMemcpyAsync(b + (size_t)k * nb, seg[k], nb, cudaMemcpyDefault, c->stream), "face copy");
   }
   CU(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  return QCB_OK;
+}
+
+int qcb_slab_faces_copy_async(qcb_lattice* L, int which, int side, int mu, int parity, void* buf, int to_face) {
+  CHECK_LAT(L);
+  if (!buf) return fail(QCB_ERR_INVALID, "null buffer");
+  if (!L->slab_tl) return fail(QCB_ERR_STATE, "not a slab");
+  if (mu < -1 || mu > 3 || parity < -1 || parity > 1) return fail(QCB_ERR_INVALID, "bad face arguments");
+  const int m0 = mu < 0 ? 0 : mu, m1 = mu < 0 ? 3 : mu;
+  const int p0 = parity < 0 ? 0 : parity, p1 = parity < 0 ? 1 : parity;
+  qcb_ctx* c = L->ctx;
+  char* b = (char*)buf;
+  for (int m = m0; m <= m1; ++m)
+    for (int p = p0; p <= p1; ++p) {
+      void* seg[9];
+      size_t nb = 0;
+      int ns = 0;
+      TRY(qcb_slab_face(L, which, side, m, p, seg, &nb, &ns));
+      LOCK(c);
+      TRY(set_device(c));
+      for (int k = 0; k < ns; ++k) {
+        if (to_face)
+          CU(cudaMemcpyAsync(seg[k], b, nb, cudaMemcpyDefault, c->stream), "face copy");
+        else
+          CU(cudaMemcpyAsync(b, seg[k], nb, cudaMemcpyDefault, c->stream), "face copy");
+        b += nb;
+      }
+    }
   return QCB_OK;
 }
 

@@ -34,6 +34,9 @@ struct qcb_lattice {
   // Wilson-flow work space, allocated on first use: two link buffers + accumulator.
   void* fw[2] = {nullptr, nullptr};
   void* fz = nullptr;
+  // Partial sums of the measuring heatbath passes, allocated on first use.
+  double* meas = nullptr;
+  size_t meas_n = 0;
   // Slab of a larger lattice (qcb_lattice_create_slab): global extents and the global time
   // of local time 1; slab_tl == 0 for a whole lattice.
   int gdims[4] = {0, 0, 0, 0};

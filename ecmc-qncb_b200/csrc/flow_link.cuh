@@ -29,6 +29,16 @@ __device__ __forceinline__ void flow_reunit(m3<R>& U, int stage) {
   }
 }
 
+// U' = exp(X) U.  12-real storage keeps rows 0 and 1 only (the FP64 re-orthonormalisation of
+// stage 3 also reads only those), so row 2 of the product is not formed.
+template <typename F, typename R>
+__device__ __forceinline__ m3<R> flow_product(const m3<R>& E, const m3<R>& U) {
+  if constexpr (F::NREAL == 12)
+    return mul_nn_rows01(E, U);
+  else
+    return mul_nn(E, U);
+}
+
 // The stage-dependent part of one link's stage: X from the force Z and the accumulator,
 // and the accumulator update.
 template <typename ACC, typename R, int MU>
@@ -65,7 +75,7 @@ __device__ __forceinline__ void flow_link(const Geom& g, const F& src, const F& 
                                           int par, uint32_t i) {
   const Coord x = cb_coord(g, par, i);
   if (!own_site(g, x.c[3])) return;  // halo slice of a slab
-  const m3<R> A = staple_sum<F, R, MU>(g, src, x, par, i);
+  const m3<R> A = staple_sum_best<F, R, MU>(g, src, x, par, i);
   const m3<R> U = src.template load<R>(MU, par, i);
   // Z = P_TA(-U A) = -P_TA(U A)
   alg8<R> Z = proj_ta(mul_nn(U, A));
@@ -73,7 +83,7 @@ __device__ __forceinline__ void flow_link(const Geom& g, const F& src, const F& 
   for (int k = 0; k < 8; ++k) Z.a[k] = -Z.a[k];
   const alg8<R> X = flow_x<ACC, R, MU>(acc, Z, eps, stage, par, i);
   const m3<R> E = exp_su3(X);
-  m3<R> Un = mul_nn(E, U);
+  m3<R> Un = flow_product<F, R>(E, U);
   flow_reunit<R>(Un, stage);
   dst.template store<R>(MU, par, i, Un);
 }
@@ -113,7 +123,7 @@ __device__ __forceinline__ void flow_link_rt(const Geom& g, const F& src, const 
     }
   }
   const m3<R> E = exp_su3(X);
-  m3<R> Un = mul_nn(E, U);
+  m3<R> Un = flow_product<F, R>(E, U);
   flow_reunit<R>(Un, stage);
   dst.template store<R>(mu, par, i, Un);
 }

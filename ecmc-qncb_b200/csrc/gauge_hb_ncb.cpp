@@ -164,8 +164,9 @@ struct Run {
   int cum[4] = {0, 0, 0, 0};  // cumulative shift not yet applied to the stored links
   std::mt19937_64 shift_rng;
 
-  // One shift of the run: N_samples * N_sweeps sweeps (heatbathcb::samples).
-  void heatbath() {
+  // One shift of the run: N_samples * N_sweeps sweeps (heatbathcb::samples); with plaq, also
+  // the mean plaquette after them (on the periodic schedule summed inside the last sweep).
+  void heatbath(double* plaq = nullptr) {
     const int n = rp.N_samples * rp.N_sweeps;
     if (ref_schedule) {
       std::uniform_int_distribution<int> rand_l_shift(0, rp.L_core - 1);
@@ -175,15 +176,13 @@ struct Run {
       const int Lg = rp.L_core * rp.n_core_dims;
       for (int d = 0; d < 4; ++d) cum[d] = (cum[d] + s[d]) % Lg;
       CHECK(qcb_heatbath_frozen(lat, rp.beta, n, rp.N_hits, key, sweep, rp.L_core, cum), "heatbath");
+      if (plaq) CHECK(qcb_plaquette(lat, plaq), "plaquette");
+    } else if (plaq) {
+      CHECK(qcb_heatbath_plaquette(lat, rp.beta, n, rp.N_hits, key, sweep, plaq), "heatbath");
     } else {
       CHECK(qcb_heatbath(lat, rp.beta, n, rp.N_hits, key, sweep), "heatbath");
     }
     sweep += (uint64_t)n;
-  }
-  double plaquette() {
-    double p = 0;
-    CHECK(qcb_plaquette(lat, &p), "plaquette");
-    return p;
   }
   std::vector<double> topo() {
     std::vector<double> tqe(3 * (size_t)rp.N_steps_gf);
@@ -233,9 +232,10 @@ void generate_hb_cb(Run& R, bool existing, int precision, int storage, int devic
   std::cout << "Thermalisation : " << rp.N_therm << " shifts\n";
   std::cout << "===========================================\n";
   for (int i = 0; i < rp.N_therm; i++) {
-    R.heatbath();
-    if (i % rp.N_shift_plaquette == 0) {
-      double p = R.plaquette();
+    double p = 0;
+    const bool meas = i % rp.N_shift_plaquette == 0;
+    R.heatbath(meas ? &p : nullptr);
+    if (meas) {
       std::cout << "====== Plaquette ======\n";
       std::cout << "(Therm) Sample " << i / rp.N_shift_plaquette << ", <P> = " << p << "\n";
     }
@@ -246,9 +246,10 @@ void generate_hb_cb(Run& R, bool existing, int precision, int storage, int devic
   std::cout << "===========================================\n";
   for (int i = 0; i < rp.N_shift; i++) {
     std::cout << "\n\n=============" << "Shift " << i << "=============\n";
-    R.heatbath();
-    if (i % rp.N_shift_plaquette == 0) {
-      double p = R.plaquette();
+    double p = 0;
+    const bool meas = i % rp.N_shift_plaquette == 0;
+    R.heatbath(meas ? &p : nullptr);
+    if (meas) {
       std::cout << "====== Plaquette ======\n";
       std::cout << "Sample " << i / rp.N_shift_plaquette << ", <P> = " << p << "\n";
       plaquette.push_back(p);

@@ -145,14 +145,14 @@ __device__ __forceinline__ bool cm_subgroup(m3<R>& U, const m3<R>& A, R beta, ui
   return true;
 }
 
-// n_hits Cabibbo-Marinari hits on link (MU, par, i) of field f; returns the number of KP
-// draws that hit the attempt cap.
-template <typename F, typename R, int NR, int MU>
-__device__ __forceinline__ uint32_t hb_update_link(const Geom& g, const F& f, int par, uint32_t i, R beta,
-                                                   uint32_t k0, uint32_t k1, uint32_t sweep, int n_hits) {
-  const Coord x = cb_coord(g, par, i);
-  if (!own_site(g, x.c[3])) return 0;  // halo slice of a slab
-  const m3<R> A = staple_sum<F, R, MU>(g, f, x, par, i);
+// n_hits Cabibbo-Marinari hits on link (MU, par, i) of field f, at site x; returns the number
+// of KP draws that hit the attempt cap.  With MEAS, *retr receives Re tr(U A) of the updated
+// (stored) link U and its staple A: the sum of Re tr of the six plaquettes that contain U.
+template <typename F, typename R, int NR, int MU, bool MEAS = false>
+__device__ __forceinline__ uint32_t hb_update_at(const Geom& g, const F& f, const Coord& x, int par, uint32_t i,
+                                                 R beta, uint32_t k0, uint32_t k1, uint32_t sweep, int n_hits,
+                                                 R* retr = nullptr) {
+  const m3<R> A = staple_sum_best<F, R, MU>(g, f, x, par, i);
   m3<R> U = f.template load<R>(MU, par, i);
   const uint32_t link = (uint32_t)MU * g.Vg + (x.s + g.soff);
   uint32_t fails = 0;
@@ -168,7 +168,16 @@ __device__ __forceinline__ uint32_t hb_update_link(const Geom& g, const F& f, in
     reunitarize_rows(U);
   }
   f.template store<R>(MU, par, i, U);
+  if constexpr (MEAS) *retr = re_tr_nn(U, A);
   return fails;
+}
+
+template <typename F, typename R, int NR, int MU>
+__device__ __forceinline__ uint32_t hb_update_link(const Geom& g, const F& f, int par, uint32_t i, R beta,
+                                                   uint32_t k0, uint32_t k1, uint32_t sweep, int n_hits) {
+  const Coord x = cb_coord(g, par, i);
+  if (!own_site(g, x.c[3])) return 0;  // halo slice of a slab
+  return hb_update_at<F, R, NR, MU>(g, f, x, par, i, beta, k0, k1, sweep, n_hits);
 }
 
 // Runtime-direction variant of hb_update_link (one code path for every mu), for the

@@ -69,10 +69,15 @@ static cudaError_t flow_impl(int stage, const LatDev& Ls, const LatDev& Ld, cons
   return cudaGetLastError();
 }
 
+#ifndef QCB_FLOW_SITE
+#define QCB_FLOW_SITE 0
+#endif
+
 cudaError_t launch_flow_stage(int stage, const LatDev& src, const LatDev& dst, const AlgDev& z, double eps,
                               cudaStream_t s, int block) {
   if (block <= 0) block = 128;
   if (src.prec != dst.prec || src.nr != dst.nr) return cudaErrorInvalidValue;
+  if (QCB_FLOW_SITE && src.prec == 1) return launch_flow_site(stage, src, dst, z, eps, s);
   QCB_DISPATCH_STORE(src, flow_impl, stage, src, dst, z, eps, s, block);
 }
 

@@ -15,6 +15,8 @@
 //   i and j only.
 #include "dispatch.cuh"
 #include "hb_link.cuh"
+#include "obs_site.cuh"
+#include "reduce.cuh"
 
 namespace qcb {
 
@@ -83,6 +85,54 @@ static cudaError_t hb_pass_impl(const LatDev& L, int mu, int par, double beta, u
     default: hb_pass_launch<S, NR, 3>(grid, block, s, L.g, f, par, S(beta), k0, k1, sweep, n_hits, status, fm); break;
   }
   return cudaGetLastError();
+}
+
+// Pass (mu = 3, par) of a measured sweep (whole lattices only): the updates of k_hb_pass, and
+// per block the FP64 sum of the spatial plaquettes of its sites (parity par), plus for par = 1
+// Re tr(U_3 A_3) of each updated link.  After the pass of parity 0 the spatial links and the
+// even U_3 links are final, so the pass of parity 1 sees final staples; every temporal
+// plaquette holds exactly one odd U_3 link, so Re tr(U_3(x) A_3(x)) over odd x counts each
+// temporal plaquette once, and the spatial plaquettes of both parities count each spatial one
+// once.
+template <typename S, int NR>
+__global__ void __launch_bounds__(128, HbMinBlocks<S>::value) k_hb_pass_meas(Geom g, Links<S, NR> f, int par, S beta,
+                                                                            uint32_t k0, uint32_t k1, uint32_t sweep,
+                                                                            int n_hits, uint32_t* status,
+                                                                            double* __restrict__ parts) {
+  __shared__ double sh[4];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  uint32_t fails = 0;
+  if (i < g.Vh) {
+    const Coord x = cb_coord(g, par, i);
+    S retr = 0;
+    fails = hb_update_at<Links<S, NR>, S, NR, 3, true>(g, f, x, par, i, beta, k0, k1, sweep, n_hits, &retr);
+    v = (double)site_plaquette_spatial<Links<S, NR>, S>(g, f, x, par, i);
+    if (par) v += (double)retr;
+  }
+  if (fails) atomicAdd(status, fails);
+  const double b = block_sum<128>(v, sh);
+  if (threadIdx.x == 0) parts[blockIdx.x] = b;
+}
+
+template <typename S, int NR>
+static cudaError_t hb_meas_impl(const LatDev& L, int par, double beta, uint64_t seed, uint32_t sweep, int n_hits,
+                                uint32_t* status, double* parts, cudaStream_t s) {
+  Links<S, NR> f;
+  f.p = reinterpret_cast<typename Links<S, NR>::V*>(L.links);
+  f.stride = L.g.stride;
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  k_hb_pass_meas<S, NR><<<grid_for(L.g.Vh, 128), 128, 0, s>>>(L.g, f, par, S(beta), k0, k1, sweep, n_hits, status,
+                                                              parts);
+  return cudaGetLastError();
+}
+
+int hb_meas_blocks(const LatDev& L) { return (int)grid_for(L.g.Vh, 128); }
+
+cudaError_t launch_hb_pass_meas(const LatDev& L, int parity, double beta, uint64_t seed, uint32_t sweep, int n_hits,
+                                uint32_t* status, double* parts, cudaStream_t s) {
+  if (L.g.tlo != 0 || L.g.thi != L.g.L[3] - 1) return cudaErrorInvalidValue;  // whole lattices only
+  QCB_DISPATCH_STORE(L, hb_meas_impl, L, parity, beta, seed, sweep, n_hits, status, parts, s);
 }
 
 cudaError_t launch_hb_pass(const LatDev& L, int mu, int parity, double beta, uint64_t seed, uint32_t sweep,

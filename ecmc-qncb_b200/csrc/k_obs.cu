@@ -12,6 +12,7 @@
 // is a fixed multiple of the SM count (grid-stride loop), so the scratch is bounded.
 #include "dispatch.cuh"
 #include "obs_site.cuh"
+#include "reduce.cuh"
 
 namespace qcb {
 
@@ -27,37 +28,6 @@ struct RedMinBlocks {
 };
 
 int reduce_blocks() { return RED_BLOCKS; }
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Block-wide sum of v (valid in thread 0).
-template <int NT>
-__device__ __forceinline__ double block_sum(double v, double* sh) {
-  v = warp_sum(v);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) sh[w] = v;
-  __syncthreads();
-  double r = 0;
-  if (w == 0) {
-    r = (lane < NT / 32) ? sh[lane] : 0.0;
-    r = warp_sum(r);
-  }
-  __syncthreads();
-  return r;
-}
-
-__device__ __forceinline__ void neumaier_add(double& s, double& c, double v) {
-  const double t = s + v;
-  if (fabs(s) >= fabs(v))
-    c += (s - t) + v;
-  else
-    c += (v - t) + s;
-  s = t;
-}
 
 // Neumaier-compensated sums of nq quantities of n partials each (parts[q*n + k]), one warp
 // per quantity: lane j sums k = j, j+32, ...; lane 0 then adds the 32 lane sums in lane
@@ -137,6 +107,29 @@ cudaError_t launch_plaquette_partials(const LatDev& L, int nblocks, double* scra
 }
 
 int reduce_threads() { return RED_THREADS; }
+
+// First level of a deterministic sum of n partials: block b sums the chunk
+// [b * chunk, min((b + 1) * chunk, n)) (thread-strided in index order, then the block tree).
+__global__ void __launch_bounds__(RED_THREADS) k_sum_chunks(const double* __restrict__ parts, int n, int chunk,
+                                                           double* __restrict__ out) {
+  __shared__ double sh[RED_THREADS / 32];
+  const int lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
+  double s = 0.0, c = 0.0;
+  for (int k = lo + threadIdx.x; k < hi; k += RED_THREADS) neumaier_add(s, c, parts[k]);
+  const double b = block_sum<RED_THREADS>(s + c, sh);
+  if (threadIdx.x == 0) out[blockIdx.x] = b;
+}
+
+// out[0] = sum of parts[0 .. n), in a fixed order whatever the device: chunks of at most
+// 256 x 128 partials per block, then the single-warp Neumaier finalize.  tmp holds 256 doubles.
+cudaError_t launch_sum_parts(const double* parts, int n, double* tmp, double* out, cudaStream_t s) {
+  if (n < 1) return cudaErrorInvalidValue;
+  const int nb = min(256, (n + RED_THREADS - 1) / RED_THREADS);
+  const int chunk = (n + nb - 1) / nb;
+  k_sum_chunks<<<nb, RED_THREADS, 0, s>>>(parts, n, chunk, tmp);
+  k_finalize<<<1, 32, 0, s>>>(tmp, nb, 1, out);
+  return cudaGetLastError();
+}
 
 template <typename S, int NR>
 __global__ void __launch_bounds__(RED_THREADS, RedMinBlocks<S>::value) k_clover_qe(Geom g, Links<S, NR> f, double* __restrict__ parts) {

@@ -48,6 +48,16 @@ cudaError_t launch_translate(const LatDev& dst, const LatDev& src, const int shi
 cudaError_t launch_hb_pass(const LatDev& L, int mu, int parity, double beta, uint64_t seed, uint32_t sweep,
                            int n_hits, uint32_t* status, cudaStream_t s, int block, const int* frozen = nullptr);
 
+// Pass (mu = 3, parity) of the last sweep of a measurement: the same updates as
+// launch_hb_pass, and one FP64 partial per block of 128 threads written to parts[0 ..
+// hb_meas_blocks(L)): the sum over the block's sites x of Re tr of the spatial plaquettes
+// P_ij(x), i < j < 3, plus for parity 1 Re tr(U_3(x) A_3(x)) with the updated link.  After
+// both parities, the partials of the two passes sum to the sum of Re tr P over all 6V
+// plaquettes of the final links.
+int hb_meas_blocks(const LatDev& L);
+cudaError_t launch_hb_pass_meas(const LatDev& L, int parity, double beta, uint64_t seed, uint32_t sweep,
+                                int n_hits, uint32_t* status, double* parts, cudaStream_t s);
+
 // ---- observables (k_obs.cu) --------------------------------------------------------
 // Reductions write per-block partial sums into scratch (nparts doubles per quantity,
 // nparts = reduce_blocks()) and a final single-block kernel writes the FP64 total(s)
@@ -58,12 +68,17 @@ cudaError_t launch_clover_qe(const LatDev& L, double* scratch, double* out2, cud
 // Plaquette sum with nblocks reduction blocks (scratch holds nblocks doubles); out[0] = sum.
 cudaError_t launch_plaquette_partials(const LatDev& L, int nblocks, double* scratch, double* out, cudaStream_t s);
 int reduce_threads();
+// out[0] = sum of parts[0 .. n) in a fixed order (two launches); tmp holds 256 doubles.
+cudaError_t launch_sum_parts(const double* parts, int n, double* tmp, double* out, cudaStream_t s);
 
 // ---- flow (k_flow.cu) --------------------------------------------------------------
 // RK3 stage k (1, 2, 3) of Luescher's integrator: reads links from src, the force
 // accumulator z, writes links to dst.
 cudaError_t launch_flow_stage(int stage, const LatDev& src, const LatDev& dst, const AlgDev& z, double eps,
                               cudaStream_t s, int block);
+// The same stage with one thread per site (k_flow_site.cu).
+cudaError_t launch_flow_site(int stage, const LatDev& src, const LatDev& dst, const AlgDev& z, double eps,
+                             cudaStream_t s);
 
 // Sets the calling thread's qcb_last_error() message; returns code.
 int set_error(int code, const char* msg);

@@ -30,6 +30,28 @@ __device__ __forceinline__ R site_plaquette(const Geom& g, const F& f, const Coo
   return sum * R(1.0 / 3.0);
 }
 
+// Sum of Re tr P_ij(x) over the spatial planes i < j < 3 (no 1/3), for the measuring
+// heatbath pass.
+template <typename F, typename R>
+__device__ __forceinline__ R site_plaquette_spatial(const Geom& g, const F& f, const Coord& x, int par,
+                                                    uint32_t i) {
+  const int opp = par ^ 1;
+  R sum = 0;
+#pragma unroll
+  for (int mu = 0; mu < 2; ++mu) {
+    const m3<R> Umu = f.template load<R>(mu, par, i);
+    const uint32_t xmu = cb_index(nb_full(g, x, mu, +1));
+#pragma unroll
+    for (int nu = mu + 1; nu < 3; ++nu) {
+      const uint32_t xnu = cb_index(nb_full(g, x, nu, +1));
+      m3<R> T1 = mul_nn(Umu, f.template load<R>(nu, opp, xmu));
+      m3<R> T2 = mul_nn(f.template load<R>(nu, par, i), f.template load<R>(mu, opp, xnu));
+      sum += re_tr_na(T1, T2);
+    }
+  }
+  return sum;
+}
+
 // ---- clover Q and E -------------------------------------------------------------------
 // Anti-Hermitian 3x3 matrix in 9 reals: F_kk = i d[k], F_ij = o[.] for (i,j) = (0,1),
 // (0,2), (1,2), and F_ji = -conj(F_ij).

@@ -195,6 +195,20 @@ __device__ __forceinline__ void acc_an(m3<R>& acc, const m3<R>& a, const m3<R>& 
       acc.e[i][j] = s;
     }
 }
+// acc += a^dagger * b^dagger
+template <typename R>
+__device__ __forceinline__ void acc_aa(m3<R>& acc, const m3<R>& a, const m3<R>& b) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      cx<R> s = acc.e[i][j];
+      s = cfma_cc(a.e[0][i], b.e[j][0], s);
+      s = cfma_cc(a.e[1][i], b.e[j][1], s);
+      s = cfma_cc(a.e[2][i], b.e[j][2], s);
+      acc.e[i][j] = s;
+    }
+}
 // Rows 0 and 1 of a * b^dagger (only rows 0 and 1 of a are read; row 2 of c is unset).
 template <typename R>
 __device__ __forceinline__ m3<R> mul_na_rows01(const m3<R>& a, const m3<R>& b) {

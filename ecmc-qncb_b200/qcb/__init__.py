@@ -367,6 +367,17 @@ class heatbathcb:
         check(lib().qcb_heatbath(field.h, float(beta), 1, int(N_hits), C.c_uint64(rng.seed), C.c_uint64(rng.sweep)))
         rng.sweep += 1
 
+    @staticmethod
+    def samples_plaquette(field: GaugeField, hp, rng: PhiloxStream) -> float:
+        """samples() followed by mean_plaquette_global(), with the plaquette summed inside the
+        last sweep (one call, no separate plaquette launch)."""
+        n = int(getattr(hp, "N_samples", 1)) * int(hp.N_sweeps)
+        out = C.c_double()
+        check(lib().qcb_heatbath_plaquette(field.h, float(hp.beta), n, int(hp.N_hits), C.c_uint64(rng.seed),
+                                           C.c_uint64(rng.sweep), C.byref(out)))
+        rng.sweep += n
+        return out.value
+
 
 class observables:
     """mpi::observables (src/observables/observables_mpi.h:9-18)."""

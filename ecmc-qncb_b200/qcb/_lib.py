@@ -131,6 +131,8 @@ SIGNATURES = {
     "qcb_load_ildg": (C.c_int, [_vp, C.c_char_p]),
     "qcb_ildg_probe": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "qcb_heatbath": (C.c_int, [_vp, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_uint64]),
+    "qcb_heatbath_plaquette": (C.c_int, [_vp, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_uint64,
+                                         C.POINTER(C.c_double)]),
     "qcb_heatbath_frozen": (C.c_int, [_vp, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_uint64, C.c_int, _ip]),
     "qcb_translate": (C.c_int, [_vp, _ip]),
     "qcb_plaquette": (C.c_int, [_vp, _dp]),
@@ -167,6 +169,7 @@ SIGNATURES = {
     "qcb_slab_face": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p),
                                 C.POINTER(C.c_size_t), _ip]),
     "qcb_slab_face_copy": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int]),
+    "qcb_slab_faces_copy_async": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int]),
     "qcb_ecmc_create": (C.c_int, [_vp, C.POINTER(EcmcParams), C.c_uint64, C.POINTER(C.c_void_p)]),
     "qcb_ecmc_destroy": (C.c_int, [_vp]),
     "qcb_ecmc_num_chains": (C.c_int, [_vp, _ip]),

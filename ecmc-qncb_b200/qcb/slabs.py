@@ -151,22 +151,38 @@ class SlabLattice:
 
 class DistSlab:
     """One slab per process of a torch.distributed group: rank r holds slab r of
-    `world` equal slabs, and the faces move to the ranks r - 1 and r + 1 (periodically)."""
+    `world` equal slabs, and the faces move to the ranks r - 1 and r + 1 (periodically).
+
+    One exchange moves every face of a pass or stage at once, ordered on the library's
+    stream: the faces of each side are packed back to back into one buffer
+    (qcb_slab_faces_copy_async), the four messages go as one batch (batch_isend_irecv), and
+    the received faces are unpacked the same way.  With the "device" transport (NCCL) the
+    host never waits: the library's stream is the current torch stream while the batch is
+    issued, so the sends start after the packs and the unpacks after the receives.  With the
+    "host" transport (gloo, pinned CPU buffers) the host waits once per exchange, for the packs,
+    before handing the buffers to gloo."""
 
     def __init__(self, ctx: Context, dims, dist, precision="fp64", storage: int = 18, transport: str = "host"):
         import torch
 
         self.dist = dist
+        self.ctx = ctx
         self.rank, self.world = dist.get_rank(), dist.get_world_size()
         self.dims = tuple(int(d) for d in dims)
         t0, tl = _split(self.dims, self.world)[self.rank]
         self.slab = Slab(ctx, self.dims, t0, tl, precision, storage)
         ns, nb = self.slab.face_shape()
         self.face_bytes = ns * nb
-        dev = "cpu" if transport == "host" else "cuda"
-        mk = (lambda: torch.empty(self.face_bytes, dtype=torch.uint8, pin_memory=True)) if dev == "cpu" else \
-            (lambda: torch.empty(self.face_bytes, dtype=torch.uint8, device="cuda"))
+        self.device = transport != "host"
+        nbytes = 8 * self.face_bytes  # all four directions and both parities
+        mk = (lambda: torch.empty(nbytes, dtype=torch.uint8, device="cuda")) if self.device else \
+            (lambda: torch.empty(nbytes, dtype=torch.uint8, pin_memory=True))
         self.buf = {k: mk() for k in ("send_lo", "send_hi", "recv_lo", "recv_hi")}
+        self.stream = torch.cuda.ExternalStream(ctx.stream) if self.device else None
+
+    def _copy(self, which, side, mu, parity, key, to_face) -> None:
+        check(lib().qcb_slab_faces_copy_async(self.slab.h, which, side, mu, parity,
+                                              C.c_void_p(self.buf[key].data_ptr()), 1 if to_face else 0))
 
     def exchange(self, which: int, mu: int = -1, parity: int = -1) -> None:
         import torch
@@ -174,26 +190,27 @@ class DistSlab:
         if self.world == 1:  # the slab is its own neighbour
             check(lib().qcb_slab_exchange(self.slab.h, self.slab.h, which, mu, parity))
             return
-        mus = range(4) if mu < 0 else [mu]
-        pars = range(2) if parity < 0 else [parity]
+        n = (4 if mu < 0 else 1) * (2 if parity < 0 else 1) * self.face_bytes
         lo, hi = (self.rank - 1) % self.world, (self.rank + 1) % self.world
         b = self.buf
-        for m in mus:
-            for p in pars:
-                # my first own slice goes to the rank below (its high halo), my last to the
-                # rank above (its low halo)
-                self.slab.face_copy(which, 1, m, p, b["send_lo"].data_ptr(), False)
-                self.slab.face_copy(which, 2, m, p, b["send_hi"].data_ptr(), False)
-                if b["send_lo"].is_cuda:
-                    torch.cuda.synchronize()
-                reqs = [self.dist.isend(b["send_lo"], lo), self.dist.isend(b["send_hi"], hi),
-                        self.dist.irecv(b["recv_hi"], hi), self.dist.irecv(b["recv_lo"], lo)]
-                for r in reqs:
-                    r.wait()
-                if b["recv_lo"].is_cuda:
-                    torch.cuda.synchronize()
-                self.slab.face_copy(which, 0, m, p, b["recv_lo"].data_ptr(), True)
-                self.slab.face_copy(which, 3, m, p, b["recv_hi"].data_ptr(), True)
+        # my first own slice goes to the rank below (its high halo), my last to the rank above
+        # (its low halo); the message order below is the matching order on every rank
+        self._copy(which, 1, mu, parity, "send_lo", False)
+        self._copy(which, 2, mu, parity, "send_hi", False)
+        ops = [self.dist.P2POp(self.dist.isend, b["send_lo"][:n], lo),
+               self.dist.P2POp(self.dist.isend, b["send_hi"][:n], hi),
+               self.dist.P2POp(self.dist.irecv, b["recv_hi"][:n], hi),
+               self.dist.P2POp(self.dist.irecv, b["recv_lo"][:n], lo)]
+        if self.device:
+            with torch.cuda.stream(self.stream):
+                for r in self.dist.batch_isend_irecv(ops):
+                    r.wait()  # orders the library stream after the receives; the host goes on
+        else:
+            self.ctx.sync()  # the packed faces are in the pinned buffers
+            for r in self.dist.batch_isend_irecv(ops):
+                r.wait()
+        self._copy(which, 0, mu, parity, "recv_lo", True)
+        self._copy(which, 3, mu, parity, "recv_hi", True)
 
     def heatbath(self, beta, n_sweeps, n_hits, seed, sweep_offset=0) -> None:
         for sw in range(n_sweeps):

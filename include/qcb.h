@@ -125,6 +125,15 @@ int qcb_ildg_probe(const char* path, uint64_t* data_offset, uint64_t* data_bytes
  * reported by the next qcb_ctx_sync / result-returning call. */
 int qcb_heatbath(qcb_lattice* lat, double beta, int n_sweeps, int n_hits, uint64_t seed,
                  uint64_t sweep_offset);
+/* mpi::heatbathcb::samples followed by mean_plaquette_global (heatbath_mpi.cpp:37-69,
+ * observables_mpi.cpp:8-43), as the driver runs them when N_shift_plaquette = 1
+ * (src/bin/gauge_hb_ncb.cpp:122-143): n_sweeps sweeps exactly as qcb_heatbath (the same
+ * links, bit for bit), then *plaq = the mean plaquette of the final links.  The plaquette is
+ * summed inside the last sweep's two mu = 3 passes, with no separate plaquette launch; it
+ * agrees with qcb_plaquette to rounding.  n_sweeps = 0 only measures.  Whole lattices only
+ * (QCB_ERR_STATE on a slab).  Synchronous. */
+int qcb_heatbath_plaquette(qcb_lattice* lat, double beta, int n_sweeps, int n_hits, uint64_t seed,
+                           uint64_t sweep_offset, double* plaq);
 /* The same sweeps with the reference's frozen links (src/geometry/GeometryCB.cpp:33-56):
  * the lattice is cut into blocks of edge l_core (one block per MPI rank in the reference)
  * and, after the field has been translated by the cumulative shift `shift` of its random
@@ -257,6 +266,13 @@ int qcb_slab_face(qcb_lattice* lat, int which, int side, int mu, int parity, voi
 /* Copies one face to (to_face = 0) or from (to_face = 1) a contiguous buffer of
  * n_segments * bytes bytes, host or device memory; synchronous. */
 int qcb_slab_face_copy(qcb_lattice* lat, int which, int side, int mu, int parity, void* buf, int to_face);
+/* The faces of every direction mu (-1: all, ascending) and every global parity (-1: both,
+ * ascending) of one side, packed back to back in buf (each face n_segments * bytes bytes, in
+ * the order of qcb_slab_face) or unpacked from it, enqueued on the context's stream without
+ * waiting: one call per side per exchange, ordered with the slab's kernels.  buf is device
+ * memory or pinned host memory that stays valid until the stream has run the copies. */
+int qcb_slab_faces_copy_async(qcb_lattice* lat, int which, int side, int mu, int parity, void* buf,
+                              int to_face);
 
 /* ---- failure detection --------------------------------------------------------------
  * The persistent batch and server kernels wait on per-lattice counters that other blocks

@@ -6,12 +6,17 @@ links of local coordinate 0 frozen in every direction d != mu (src/geometry/Geom
 a random translation of the field before every sweep (src/mpi/Shift.cpp:163-186), a
 lexicographic Cabibbo-Marinari sweep with N_hits = 1 (src/heatbath/heatbath_mpi.cpp:11-69,
 src/heatbath/heatbath.cpp:8-44), every draw from one std::mt19937_64 seeded per chain, and
-the reference's Householder hot start.  For each lattice size and beta, several independent
+a cold start (every link the identity).  For each lattice size and beta, several independent
 chains run; after n_therm discarded sweeps the plaquette of every sweep is recorded.  The
 file keeps, per chain, tau_int and the means of bins of at least 10 tau_int sweeps, so a test
-recomputes the pooled mean and its error from the file alone.
+recomputes the mean and its error from the file alone.
 
-Run from the repository root (about 10 minutes on 8 cores):
+Cold starts: on these small lattices beta 6.0 and 6.2 (and 5.7 on 4^4) lie at or above the
+finite-box deconfinement transition, where a hot start can leave a chain in a metastable state
+with twisted Polyakov-loop sectors (a lower plaquette) for far longer than one chain; an
+ordered start samples one sector, and all sectors have the same plaquette distribution.
+
+Run from the repository root (about 20 minutes on 8 cores):
     python tests/golden/make_ref_schedule_plaquette.py
 """
 import json
@@ -24,7 +29,7 @@ ROOT = HERE.parent.parent
 OUT = HERE / "ref_schedule_plaquette.json"
 
 # (L, n_chains, n_therm, n_sweeps) per lattice size; betas of the statistical oracle.
-SIZES = [(4, 8, 500, 40000), (8, 8, 300, 5000)]
+SIZES = [(4, 8, 2000, 40000), (8, 16, 1000, 5000)]
 BETAS = [5.7, 6.0, 6.2]
 # Bins are lengthened by a whole factor until a case has at most this many (longer bins are
 # still at least 10 tau_int), which keeps the file small.
@@ -40,7 +45,7 @@ def run_chain(args):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
 
-    c = oracle.RefChain(L, seed_of(L, beta, chain), False)
+    c = oracle.RefChain(L, seed_of(L, beta, chain), True)
     c.run(beta, n_therm, 1, 1)
     return (L, beta, chain), c.run(beta, n_sweeps, 1, 1)
 
@@ -49,7 +54,7 @@ def main():
     sys.path.insert(0, str(ROOT / "oracle"))
     sys.path.insert(0, str(ROOT / "tests"))
     import oracle
-    from stats import chains_summary
+    from stats import between_chain_err, chains_summary
 
     oracle.build()
     jobs = [(L, b, k, th, n) for (L, nc, th, n) in SIZES for b in BETAS for k in range(nc)]
@@ -59,7 +64,7 @@ def main():
             series[key] = x
             print("done", key, flush=True)
     out = {"generator": "tests/golden/make_ref_schedule_plaquette.py", "schedule": "reference (frozen links, "
-           "random shift per sweep, lexicographic sweep, mt19937_64, Householder hot start)", "cases": []}
+           "random shift per sweep, lexicographic sweep, mt19937_64, cold start)", "cases": []}
     for (L, nc, th, n) in SIZES:
         for b in BETAS:
             chains = [series[(L, b, k)] for k in range(nc)]
@@ -74,7 +79,7 @@ def main():
                 "tau_int": [round(t, 3) for t in s["tau_int"]],
                 "bin_length": s["bin_length"],
                 "bins": [[round(float(v), 10) for v in c] for c in s["bins"]],
-                "mean": s["mean"], "err": s["err"],
+                "mean": s["mean"], "err": s["err"], "err_between_chains": between_chain_err(s["bins"]),
             })
             print(f"L={L} beta={b}: {s['mean']:.6f} +- {s['err']:.6f}, tau_int max "
                   f"{max(s['tau_int']):.2f}, bin {s['bin_length']}, {s['n_bins']} bins")

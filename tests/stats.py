@@ -63,3 +63,17 @@ def chains_summary(series, factor: float = 10.0, length: int = 0) -> dict:
     bins = [chain_bins(x, length) for x in series]
     mean, err, nb = pooled_mean_err(bins)
     return {"tau_int": taus, "bin_length": length, "bins": bins, "mean": mean, "err": err, "n_bins": nb}
+
+
+def between_chain_err(bins_per_chain) -> float:
+    """Standard error of the grand mean from the scatter of the chain means (every chain has
+    bins of the same length).  Unlike the pooled-bin error it also sees modes slower than one
+    chain's length, such as metastable states a chain starts in and keeps."""
+    m = np.array([np.mean(c) for c in bins_per_chain])
+    return float(m.std(ddof=1) / np.sqrt(m.size))
+
+
+def chains_estimate(bins_per_chain):
+    """Mean and the larger of the pooled-bin and between-chain errors."""
+    mean, err, nb = pooled_mean_err(bins_per_chain)
+    return mean, max(err, between_chain_err(bins_per_chain)), nb

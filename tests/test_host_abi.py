@@ -42,6 +42,7 @@ def test_null_arguments_are_rejected():
     assert b"null" in L.qcb_last_error()
     assert L.qcb_plaquette(None, None) == 1
     assert L.qcb_heatbath(None, 6.0, 1, 1, 0, 0) == 1
+    assert L.qcb_heatbath_plaquette(None, 6.0, 1, 1, 0, 0, None) == 1
     assert L.qcb_ecmc_set_lanes(None, 3) == 1
     assert L.qcb_ecmc_lanes(None, None) == 1
     assert L.qcb_ecmc_sample_n(None, None, 1) == 1

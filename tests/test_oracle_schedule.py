@@ -42,13 +42,13 @@ def test_shift_sequence_range_and_determinism():
 def test_fixture_chain_reproduced_by_the_oracle():
     """The first recorded sweeps of one fixture chain come out of the oracle again: the
     fixture's bins of the 4^4, beta = 6.0 case start with the mean of the first bin of
-    chain 0 after n_therm discarded sweeps."""
+    chain 0 (cold start) after n_therm discarded sweeps."""
     import json
     from pathlib import Path
 
     gold = json.loads((Path(__file__).resolve().parent / "golden" / "ref_schedule_plaquette.json").read_text())
     case = next(c for c in gold["cases"] if c["L"] == 4 and c["beta"] == 6.0)
-    chain = orc.RefChain(4, case["seeds"][0], False)
+    chain = orc.RefChain(4, case["seeds"][0], True)
     chain.run(6.0, case["n_therm"], 1, 1)
     x = chain.run(6.0, case["bin_length"], 1, 1)
     assert abs(x.mean() - case["bins"][0][0]) < 1e-9
