@@ -81,7 +81,7 @@ int upload_layout(qcb_batch* b) {
   for (int l = 0; l < n; ++l) {
     const qcb_lattice* L = b->lats[l];
     const uint32_t nth = ceil_div(L->dev.g.Vh, b->hb_tile[l]);
-    const uint32_t ntf = 8 * ceil_div(L->dev.g.Vh, b->flow_tile[l]);
+    const uint32_t ntf = flow_items_per_tile(L->dev.prec) * ceil_div(L->dev.g.Vh, b->flow_tile[l]);
     ph[l + 1] = ph[l] + nth;
     pf[l + 1] = pf[l] + ntf;
     pr[l + 1] = pr[l] + ceil_div(L->dev.g.V, (uint32_t)batch_red_sites());
@@ -145,7 +145,7 @@ void flow_tiles_into(qcb_batch* b, int set, std::vector<BatchLat>& out) {
   out.assign(b->h_desc + set * b->n, b->h_desc + (set + 1) * b->n);
   for (int l = 0; l < b->n; ++l) {
     out[l].tile = b->flow_tile[l];
-    out[l].ntiles = 8 * ceil_div(out[l].g.Vh, b->flow_tile[l]);
+    out[l].ntiles = flow_items_per_tile(b->prec) * ceil_div(out[l].g.Vh, b->flow_tile[l]);
   }
 }
 
@@ -610,7 +610,7 @@ extern "C" int qcb_batch_autotune(qcb_batch* b, const char* cache_path) {
           d.beta = 6.0;
           d.k0 = 12345u;
           d.tile = (uint32_t)cand;
-          d.ntiles = (kind == 0 ? 1u : 8u) * ceil_div(d.g.Vh, (uint32_t)cand);
+          d.ntiles = (kind == 0 ? 1u : flow_items_per_tile(L->dev.prec)) * ceil_div(d.g.Vh, (uint32_t)cand);
           pre[j + 1] = pre[j] + d.ntiles;
         }
         if (cand > 2 * (int)dsc[0].g.Vh && cand != cands[0]) continue;  // larger than the lattice

@@ -17,7 +17,7 @@ struct BatchLat {
   uint32_t k0, k1;  // Philox key (seed)
   uint32_t sweep0;  // sweep counter of the launch's first sweep
   uint32_t tile;    // sites per work item (any multiple of the block size)
-  uint32_t ntiles;  // work items of this lattice per level (flow: 8 x site tiles)
+  uint32_t ntiles;  // work items of this lattice per level (flow: flow_items_per_tile x site tiles)
   uint32_t nlev;    // levels this lattice takes part in (0 = all levels of the launch)
   int kind;         // BATCH_HB or BATCH_FLOW (mixed launches); BATCH_NONE: no work
   int n_hits;       // heatbath hits (0 = the launch's value)
@@ -38,6 +38,11 @@ struct BatchRun {
 };
 
 enum : int { BATCH_NONE = -1, BATCH_HB = 0, BATCH_FLOW = 1, BATCH_MIXED = 2 };
+
+// Work items of one flow level per tile of sites: FP32 lattices run one thread per site (both
+// parities, 2 items), FP64 lattices one thread per link (4 directions x 2 parities, 8 items),
+// as the single-lattice flow does, so that batched and single results stay bit-identical.
+inline uint32_t flow_items_per_tile(int prec) { return prec == 1 ? 2u : 8u; }
 
 // Cooperative persistent launch (kind BATCH_HB, BATCH_FLOW or BATCH_MIXED): the grid is the
 // co-resident maximum (capped by max_blocks when > 0) for the given block size.

@@ -20,6 +20,7 @@
 #include "batch.h"
 #include "dispatch.cuh"
 #include "flow_link.cuh"
+#include "flow_site.cuh"
 #include "hb_link.cuh"
 #include "obs_site.cuh"
 #include "sync.cuh"
@@ -88,14 +89,17 @@ __device__ __forceinline__ uint32_t hb_item(const BatchRun& run, const BatchLat&
 }
 
 // Flow level j = 3 s + k is stage k of RK3 step s.  With a = links, b = work for even s
-// (swapped for odd s): stage 0 a -> b, stage 1 b -> a, stage 2 a -> b.  A flow item covers a
-// tile of one (mu, parity) block: item r of a lattice -> (mu, parity) = r % 8, tile = r / 8.
-// The direction and the stage are run-time values here (one code body for all twelve
-// (mu, stage) pairs): compiled-direction bodies, with the items of a level ordered
+// (swapped for odd s): stage 0 a -> b, stage 1 b -> a, stage 2 a -> b.  FP32: a flow item
+// covers a tile of sites of one parity, all four links of each site (the single-lattice site
+// kernel's body, flow_site.cuh): item r -> parity r % 2, tile r / 2.  FP64: a flow item covers
+// a tile of one (mu, parity) block, one link per thread: item r -> (mu, parity) = r % 8,
+// tile = r / 8.  The direction and the stage are run-time values here (one code body for all
+// twelve (mu, stage) pairs): compiled-direction bodies, with the items of a level ordered
 // direction-major, measured 7% (heatbath) and 13% (flow) slower on the 64-lattice batch,
 // from register spills and instruction-cache misses.
 template <typename S, int NR>
-__device__ __forceinline__ void flow_item(const BatchRun& run, const BatchLat& B, uint32_t level, uint32_t local) {
+__device__ __forceinline__ void flow_item(const BatchRun& run, const BatchLat& B, uint32_t level, uint32_t local,
+                                          S* slot_mem) {
   typedef Links<S, NR, LD_CG> F;
   typedef AlgField<S, LD_CG> Z;
   const uint32_t step = level / 3, stage = level - 3 * step;
@@ -109,12 +113,22 @@ __device__ __forceinline__ void flow_item(const BatchRun& run, const BatchLat& B
   acc.p = reinterpret_cast<typename Z::V*>(B.acc);
   acc.stride = B.g.stride;
   const S eps = S(B.eps != 0.0 ? B.eps : run.eps);
-  const int mp8 = (int)(local & 7), mu = mp8 >> 1, par = mp8 & 1;
-  const uint32_t tile = local >> 3;
-  for (uint32_t k = threadIdx.x; k < B.tile; k += blockDim.x) {
-    const uint32_t i = tile * B.tile + k;
-    if (i >= B.g.Vh) break;
-    flow_link_rt<F, Z, S>(B.g, src, dst, acc, eps, (int)stage + 1, mu, par, i);
+  if constexpr (sizeof(S) == 4) {
+    const int par = (int)(local & 1);
+    const uint32_t tile = local >> 1;
+    for (uint32_t k = threadIdx.x; k < B.tile; k += blockDim.x) {
+      const uint32_t i = tile * B.tile + k;
+      if (i >= B.g.Vh) break;
+      flow_site<F, Z, S, NR>(B.g, src, dst, acc, eps, (int)stage + 1, par, i, slot_mem);
+    }
+  } else {
+    const int mp8 = (int)(local & 7), mu = mp8 >> 1, par = mp8 & 1;
+    const uint32_t tile = local >> 3;
+    for (uint32_t k = threadIdx.x; k < B.tile; k += blockDim.x) {
+      const uint32_t i = tile * B.tile + k;
+      if (i >= B.g.Vh) break;
+      flow_link_rt<F, Z, S>(B.g, src, dst, acc, eps, (int)stage + 1, mu, par, i);
+    }
   }
 }
 
@@ -125,6 +139,7 @@ __device__ __forceinline__ void flow_item(const BatchRun& run, const BatchLat& B
 // a lattice of kind BATCH_NONE in a mixed launch takes part in none.
 template <typename S, int NR, int KINDS>
 __global__ void __launch_bounds__(128, sizeof(S) == 4 ? QCB_BATCH_MINB32 : 2) k_batch(BatchRun run) {
+  extern __shared__ __align__(16) unsigned char kb_smem[];  // FP32 flow: the T slots of flow_site
   const uint64_t total = (uint64_t)run.nlevels * run.per_level;
   uint32_t fails = 0;
   for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
@@ -140,7 +155,7 @@ __global__ void __launch_bounds__(128, sizeof(S) == 4 ? QCB_BATCH_MINB32 : 2) k_
     if (kind == BATCH_HB)
       fails += hb_item<S, NR>(run, B, level, local);
     else
-      flow_item<S, NR>(run, B, level, local);
+      flow_item<S, NR>(run, B, level, local, reinterpret_cast<S*>(kb_smem));
     block_release(&run.done[l]);
   }
   if (fails) atomicAdd(&run.status[0], fails);
@@ -151,8 +166,9 @@ template <typename S, int NR>
 static cudaError_t batch_launch_impl(int kind, const BatchRun& run, int block, int max_blocks, cudaStream_t s) {
   void* fn = (kind == BATCH_HB) ? (void*)k_batch<S, NR, BATCH_HB>
              : (kind == BATCH_FLOW) ? (void*)k_batch<S, NR, BATCH_FLOW> : (void*)k_batch<S, NR, BATCH_MIXED>;
+  const size_t smem = (sizeof(S) == 4 && kind != BATCH_HB) ? flow_site_smem<S, NR>() : 0;
   int per_sm = 0, dev = 0, sms = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem);
   if (e != cudaSuccess) return e;
   e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -166,7 +182,7 @@ static cudaError_t batch_launch_impl(int kind, const BatchRun& run, int block, i
   if (grid == 0) return cudaSuccess;
   BatchRun r = run;
   void* args[] = {&r};
-  return cudaLaunchCooperativeKernel(fn, dim3((unsigned)grid), dim3(block), args, 0, s);
+  return cudaLaunchCooperativeKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, s);
 }
 
 cudaError_t launch_batch(int kind, const BatchRun& run, int prec, int nr, int block, int max_blocks,

@@ -3,153 +3,26 @@
 // Reference: GradientFlow (src/flow/gradient_flow.cpp:15-114), as in k_flow.cu; the stage
 // arithmetic per link is the same (flow_link.cuh), only the work is grouped by site.
 //
-// A thread updates the four links U_mu(x), mu = 0..3, of its site in turn, so the links
-// around x are read while they are in L1/L2 (the per-direction kernels stream the neighbour
-// links of every direction from DRAM once per direction), and the product the forward
-// staples of U_mu(x) and U_nu(x) share is formed once: with
-//   T_{mu nu} = U_nu(x+mu) U_mu(x+nu)^dagger,
-// the forward staple of U_mu(x) in plane nu is T_{mu nu} U_nu(x)^dagger and that of U_nu(x)
-// in plane mu is T_{mu nu}^dagger U_mu(x)^dagger.  T_{mu nu} (mu < nu) is formed while U_mu(x)
-// is updated and kept in shared memory (private to the thread) until U_nu(x) uses it: the
-// six products of a site need four slots at most (slot 0: T01, then T12; slot 1: T02, then
-// T23; slot 2: T03; slot 3: T13), because the planes are visited with nu ascending.
-// The direction and plane loops are not unrolled: one code body serves every (mu, nu).
+// One thread per site; the per-site body (flow_site.cuh) forms the product shared by the two
+// forward staples of each plane once and keeps the links around x in L1/L2.
 #include "dispatch.cuh"
-#include "flow_link.cuh"
+#include "flow_site.cuh"
 
 namespace qcb {
 
-constexpr int FS_THREADS = 128;
 #ifndef QCB_FLOW_SITE_MINB
 #define QCB_FLOW_SITE_MINB 5
 #endif
-
-// Slot of T_{a b}, a < b, as 4-bit fields indexed by 4a + b.
-__device__ __forceinline__ int t_slot(int a, int b) {
-  constexpr unsigned long long tbl = (0ull << 4) | (1ull << 8) | (2ull << 12) | (0ull << 24) | (3ull << 28) | (1ull << 44);
-  return (int)((tbl >> (4 * (4 * a + b))) & 0xF);
-}
-
-template <typename R, int TS>
-struct TSlots {
-  R* base;  // [4][TS][FS_THREADS]
-  __device__ __forceinline__ R* at(int slot, int k) const { return base + (slot * TS + k) * FS_THREADS + threadIdx.x; }
-  __device__ __forceinline__ void put(int slot, const m3<R>& t) const {
-#pragma unroll
-    for (int r = 0; r < TS / 6; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        *at(slot, 6 * r + 2 * c) = t.e[r][c].re;
-        *at(slot, 6 * r + 2 * c + 1) = t.e[r][c].im;
-      }
-  }
-  __device__ __forceinline__ m3<R> get(int slot) const {
-    m3<R> t;
-#pragma unroll
-    for (int r = 0; r < TS / 6; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) t.e[r][c] = mk<R>(*at(slot, 6 * r + 2 * c), *at(slot, 6 * r + 2 * c + 1));
-    if (TS == 12) reconstruct_row2(t);
-    return t;
-  }
-};
 
 template <typename S, int NR, int STAGE>
 __global__ void __launch_bounds__(FS_THREADS, QCB_FLOW_SITE_MINB) k_flow_site(Geom g, Links<S, NR> src,
                                                                              Links<S, NR> dst, AlgField<S> acc,
                                                                              S eps) {
-  typedef S R;
-  constexpr int TS = NR == 12 ? 12 : 18;
   extern __shared__ __align__(16) unsigned char fs_smem[];
-  const TSlots<R, TS> slots{reinterpret_cast<R*>(fs_smem)};
-  const int par = blockIdx.x & 1, opp = par ^ 1;
+  const int par = blockIdx.x & 1;
   const uint32_t i = (blockIdx.x >> 1) * FS_THREADS + threadIdx.x;
   if (i >= g.Vh) return;
-  const Coord x = cb_coord(g, par, i);
-  if (!own_site(g, x.c[3])) return;  // halo slice of a slab
-  const NbOff o = nb_offsets(g, x);
-#pragma unroll 1
-  for (int mu = 0; mu < 4; ++mu) {
-    const int32_t upmu = sel4(o.up, mu);
-    const uint32_t ixmu = cb_index((uint32_t)((int32_t)x.s + upmu));
-    m3<R> A;
-    set_zero(A);
-#pragma unroll 1
-    for (int k = 0; k < 3; ++k) {
-      const int nu = k + (k >= mu);
-      const int32_t upnu = sel4(o.up, nu), dnnu = sel4(o.dn, nu);
-      const uint32_t ixnu = cb_index((uint32_t)((int32_t)x.s + upnu));
-      const uint32_t ixmnu = cb_index((uint32_t)((int32_t)x.s + dnnu));
-      const uint32_t ixmunu = cb_index((uint32_t)((int32_t)x.s + upmu + dnnu));
-      // forward: T_{mu nu} U_nu(x)^dagger, T shared with the plane's other link
-      {
-        const m3<R> U2 = src.template load<R>(nu, par, i);
-        if (nu > mu) {
-          m3<R> T;
-          if constexpr (NR == 12) {
-            const m3<R> U0 = src.template load_rows01<R>(nu, opp, ixmu);
-            const m3<R> U1 = src.template load<R>(mu, opp, ixnu);
-            T = mul_na_rows01(U0, U1);
-            slots.put(t_slot(mu, nu), T);
-            reconstruct_row2(T);
-          } else {
-            T = mul_na(src.template load<R>(nu, opp, ixmu), src.template load<R>(mu, opp, ixnu));
-            slots.put(t_slot(mu, nu), T);
-          }
-          acc_na(A, T, U2);
-        } else {
-          const m3<R> T = slots.get(t_slot(nu, mu));  // T_{nu mu} = T_{mu nu}^dagger
-          acc_aa(A, T, U2);
-        }
-      }
-      // backward: (U_mu(x-nu) U_nu(x+mu-nu))^dagger U_nu(x-nu)
-      if constexpr (NR == 12) {
-        const m3<R> V1 = src.template load_rows01<R>(mu, opp, ixmnu);
-        const m3<R> V0 = src.template load<R>(nu, par, ixmunu);
-        m3<R> P = mul_nn_rows01(V1, V0);
-        reconstruct_row2(P);
-        const m3<R> V2 = src.template load<R>(nu, opp, ixmnu);
-        acc_an(A, P, V2);
-      } else {
-        const m3<R> V0 = src.template load<R>(nu, par, ixmunu);
-        const m3<R> V1 = src.template load<R>(mu, opp, ixmnu);
-        const m3<R> P = mul_aa(V0, V1);
-        const m3<R> V2 = src.template load<R>(nu, opp, ixmnu);
-        acc_nn(A, P, V2);
-      }
-    }
-    const m3<R> U = src.template load<R>(mu, par, i);
-    alg8<R> Z = proj_ta(mul_nn(U, A));
-#pragma unroll
-    for (int q = 0; q < 8; ++q) Z.a[q] = -Z.a[q];
-    alg8<R> X;
-    if (STAGE == 1) {
-      const R c = R(0.25) * eps;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) X.a[q] = c * Z.a[q];
-      acc.template store<R>(mu, par, i, Z);
-    } else {
-      const alg8<R> Z0 = acc.template load<R>(mu, par, i);
-      if (STAGE == 2) {
-        const R c1 = R(8.0 / 9.0) * eps, c0 = R(17.0 / 36.0) * eps;
-        alg8<R> N;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          X.a[q] = c1 * Z.a[q] - c0 * Z0.a[q];
-          N.a[q] = R(8.0 / 9.0) * Z.a[q] - R(17.0 / 36.0) * Z0.a[q];
-        }
-        acc.template store<R>(mu, par, i, N);
-      } else {
-        const R c1 = R(0.75) * eps;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) X.a[q] = c1 * Z.a[q] - eps * Z0.a[q];
-      }
-    }
-    const m3<R> E = exp_su3(X);
-    m3<R> Un = flow_product<Links<S, NR>, R>(E, U);
-    flow_reunit<R>(Un, STAGE);
-    dst.template store<R>(mu, par, i, Un);
-  }
+  flow_site<Links<S, NR>, AlgField<S>, S, NR>(g, src, dst, acc, eps, STAGE, par, i, reinterpret_cast<S*>(fs_smem));
 }
 
 template <typename S, int NR>
@@ -163,8 +36,7 @@ static cudaError_t flow_site_impl(int stage, const LatDev& Ls, const LatDev& Ld,
   AlgField<S> acc;
   acc.p = reinterpret_cast<typename AlgField<S>::V*>(z.p);
   acc.stride = Ls.g.stride;
-  constexpr int TS = NR == 12 ? 12 : 18;
-  const size_t smem = (size_t)4 * TS * FS_THREADS * sizeof(S);
+  const size_t smem = flow_site_smem<S, NR>();
   dim3 grid(grid_for(Ls.g.Vh, FS_THREADS) * 2);
   cudaError_t e = cudaSuccess;
   if (stage == 1) {

@@ -212,7 +212,7 @@ cudaError_t tick(qcb_server* s, std::vector<Job*>& act, std::vector<int>& finish
       d.links = odd ? j->fw1 : j->fw0;
       d.work = odd ? j->fw0 : j->fw1;
       d.acc = j->acc;
-      d.ntiles = 8u * cdiv(d.g.Vh, tile);
+      d.ntiles = flow_items_per_tile(s->cfg.precision) * cdiv(d.g.Vh, tile);
       d.nlev = 3u * (uint32_t)q;
       d.eps = j->spec.eps;
     }
