@@ -118,6 +118,37 @@ int rk3(qcb_lattice* L, const LatDev& a, const LatDev& b, double eps) {
   return QCB_OK;
 }
 
+// Device buffer of at least `need` doubles for the partial sums of fused measurements.
+int ensure_meas(qcb_lattice* L, size_t need) {
+  if (L->meas_n >= need) return QCB_OK;
+  cudaFree(L->meas);
+  L->meas = nullptr;
+  L->meas_n = 0;
+  if (cudaMalloc(&L->meas, need * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(QCB_ERR_NOMEM, "cannot allocate the measurement partial sums");
+  }
+  L->meas_n = need;
+  return QCB_OK;
+}
+
+// One RK3 step a -> b as rk3(), with the clover (Q, E) of the step's input summed inside
+// stage 1 and written to dst_dev[0..1] (FP32 whole lattices: one thread per site).
+int rk3_qe(qcb_lattice* L, const LatDev& a, const LatDev& b, double eps, double* dst_dev) {
+  qcb_ctx* c = L->ctx;
+  AlgDev z;
+  z.p = L->fz;
+  const int nb = flow_site_blocks(a);
+  const int r_ = ensure_meas(L, 2 * (size_t)nb + 512);
+  if (r_ != QCB_OK) return r_;
+  CU(launch_flow_site_qe(a, b, z, eps, L->meas, c->stream), "flow stage 1 with Q/E");
+  CU(launch_qe_from_parts(L->meas, nb, L->meas + 2 * nb, dst_dev, 1.0 / (double)a.g.Vg, c->stream), "Q/E sums");
+  CU(launch_flow_stage(2, b, a, z, eps, c->stream, c->block), "flow stage 2");
+  CU(launch_flow_stage(3, a, b, z, eps, c->stream, c->block), "flow stage 3");
+  c->launches += 6;
+  return QCB_OK;
+}
+
 int qe_async(qcb_lattice* L, const LatDev& d, double* dst_dev) {
   qcb_ctx* c = L->ctx;
   CU(launch_clover_qe(d, c->d_scratch, dst_dev, c->stream, c->block), "clover Q/E");
@@ -688,17 +719,7 @@ int qcb_heatbath_plaquette(qcb_lattice* L, double beta, int n_sweeps, int n_hits
     c->launches += 2;
   } else {
     const int nb = hb_meas_blocks(L->dev);
-    const size_t need = 2 * (size_t)nb + 256;
-    if (L->meas_n < need) {
-      cudaFree(L->meas);
-      L->meas = nullptr;
-      L->meas_n = 0;
-      if (cudaMalloc(&L->meas, need * sizeof(double)) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(QCB_ERR_NOMEM, "cannot allocate the measurement partial sums");
-      }
-      L->meas_n = need;
-    }
+    TRY(ensure_meas(L, 2 * (size_t)nb + 256));
     for (int s = 0; s < n_sweeps; ++s) {
       const uint32_t sweep = (uint32_t)(sweep_offset + (uint64_t)s);
       const bool last = s == n_sweeps - 1;
@@ -821,9 +842,15 @@ int qcb_flow_measure(qcb_lattice* L, double eps, int n_steps_gf, int n_rk_steps,
     std::vector<double> ts(n);
     for (int k = 0; k < n; ++k) {
       ts[k] = t;
-      TRY(qe_async(L, a, c->d_out + 2 * k));
+      // FP32: the record is summed inside stage 1 of the group's first RK3 step, which reads
+      // the same links; otherwise (FP64, or no step follows) by the clover kernel.
+      const bool fused = a.prec == QCB_FP32 && n_rk_steps > 0;
+      if (!fused) TRY(qe_async(L, a, c->d_out + 2 * k));
       for (int r = 0; r < n_rk_steps; ++r) {
-        TRY(rk3(L, a, b, eps));
+        if (fused && r == 0)
+          TRY(rk3_qe(L, a, b, eps, c->d_out + 2 * k));
+        else
+          TRY(rk3(L, a, b, eps));
         LatDev tmp = a;
         a = b;
         b = tmp;

@@ -7,6 +7,8 @@
 // forward staples of each plane once and keeps the links around x in L1/L2.
 #include "dispatch.cuh"
 #include "flow_site.cuh"
+#include "obs_site.cuh"
+#include "reduce.cuh"
 
 namespace qcb {
 
@@ -23,6 +25,63 @@ __global__ void __launch_bounds__(FS_THREADS, QCB_FLOW_SITE_MINB) k_flow_site(Ge
   const uint32_t i = (blockIdx.x >> 1) * FS_THREADS + threadIdx.x;
   if (i >= g.Vh) return;
   flow_site<Links<S, NR>, AlgField<S>, S, NR>(g, src, dst, acc, eps, STAGE, par, i, reinterpret_cast<S*>(fs_smem));
+}
+
+// Stage 1 of a measured RK3 step: the site's four links as k_flow_site, and the clover q and e
+// of the site from the same source links (site_qe, the arithmetic of k_clover_qe), summed per
+// block in FP64.  The clover's links are the stage's own neighbourhood, read from L1/L2.
+// Four resident blocks (128 registers): the clover planes spill at the flow kernel's bound of 96.
+template <typename S, int NR>
+__global__ void __launch_bounds__(FS_THREADS, 4) k_flow_site_qe(Geom g, Links<S, NR> src,
+                                                                                Links<S, NR> dst, AlgField<S> acc,
+                                                                                S eps, double* __restrict__ parts) {
+  extern __shared__ __align__(16) unsigned char fs_smem[];
+  __shared__ double sh[FS_THREADS / 32];
+  const int par = blockIdx.x & 1;
+  const uint32_t i = (blockIdx.x >> 1) * FS_THREADS + threadIdx.x;
+  double q = 0.0, e = 0.0;
+  if (i < g.Vh) {
+    flow_site<Links<S, NR>, AlgField<S>, S, NR>(g, src, dst, acc, eps, 1, par, i, reinterpret_cast<S*>(fs_smem));
+    const Coord x = cb_coord(g, par, i);
+    S qs = 0, es = 0;
+    site_qe<Links<S, NR>, S>(g, src, x, par, i, &qs, &es);
+    q = (double)qs;
+    e = (double)es;
+  }
+  const double bq = block_sum<FS_THREADS>(q, sh);
+  const double be = block_sum<FS_THREADS>(e, sh);
+  if (threadIdx.x == 0) {
+    parts[blockIdx.x] = bq;
+    parts[gridDim.x + blockIdx.x] = be;
+  }
+}
+
+template <typename S, int NR>
+static cudaError_t flow_site_qe_impl(const LatDev& Ls, const LatDev& Ld, const AlgDev& z, double eps, double* parts,
+                                     cudaStream_t s) {
+  Links<S, NR> src, dst;
+  src.p = reinterpret_cast<typename Links<S, NR>::V*>(Ls.links);
+  src.stride = Ls.g.stride;
+  dst.p = reinterpret_cast<typename Links<S, NR>::V*>(Ld.links);
+  dst.stride = Ld.g.stride;
+  AlgField<S> acc;
+  acc.p = reinterpret_cast<typename AlgField<S>::V*>(z.p);
+  acc.stride = Ls.g.stride;
+  const size_t smem = flow_site_smem<S, NR>();
+  k_flow_site_qe<S, NR><<<dim3(grid_for(Ls.g.Vh, FS_THREADS) * 2), FS_THREADS, smem, s>>>(Ls.g, src, dst, acc, S(eps),
+                                                                                        parts);
+  return cudaGetLastError();
+}
+
+int flow_site_blocks(const LatDev& L) { return (int)grid_for(L.g.Vh, FS_THREADS) * 2; }
+
+cudaError_t launch_flow_site_qe(const LatDev& src, const LatDev& dst, const AlgDev& z, double eps, double* parts,
+                                cudaStream_t s) {
+  if (src.prec != dst.prec || src.nr != dst.nr || src.prec != QCB_PREC_FP32) return cudaErrorInvalidValue;
+  if (src.g.tlo != 0 || src.g.thi != src.g.L[3] - 1) return cudaErrorInvalidValue;  // whole lattices only
+  if (src.nr == 12) return flow_site_qe_impl<float, 12>(src, dst, z, eps, parts, s);
+  if (src.nr == 18) return flow_site_qe_impl<float, 18>(src, dst, z, eps, parts, s);
+  return cudaErrorInvalidValue;
 }
 
 template <typename S, int NR>

@@ -108,27 +108,34 @@ cudaError_t launch_plaquette_partials(const LatDev& L, int nblocks, double* scra
 
 int reduce_threads() { return RED_THREADS; }
 
-// First level of a deterministic sum of n partials: block b sums the chunk
-// [b * chunk, min((b + 1) * chunk, n)) (thread-strided in index order, then the block tree).
+// First level of a deterministic sum of nq quantities of n partials each (quantity q at
+// parts[q * n ..]): block (b, q) sums the chunk [b * chunk, min((b + 1) * chunk, n)) of quantity
+// q (thread-strided in index order, then the block tree) into out[q * gridDim.x + b].
 __global__ void __launch_bounds__(RED_THREADS) k_sum_chunks(const double* __restrict__ parts, int n, int chunk,
                                                            double* __restrict__ out) {
   __shared__ double sh[RED_THREADS / 32];
+  const double* p = parts + (size_t)blockIdx.y * n;
   const int lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
   double s = 0.0, c = 0.0;
-  for (int k = lo + threadIdx.x; k < hi; k += RED_THREADS) neumaier_add(s, c, parts[k]);
+  for (int k = lo + threadIdx.x; k < hi; k += RED_THREADS) neumaier_add(s, c, p[k]);
   const double b = block_sum<RED_THREADS>(s + c, sh);
-  if (threadIdx.x == 0) out[blockIdx.x] = b;
+  if (threadIdx.x == 0) out[blockIdx.y * gridDim.x + blockIdx.x] = b;
 }
 
-// out[0] = sum of parts[0 .. n), in a fixed order whatever the device: chunks of at most
-// 256 x 128 partials per block, then the single-warp Neumaier finalize.  tmp holds 256 doubles.
-cudaError_t launch_sum_parts(const double* parts, int n, double* tmp, double* out, cudaStream_t s) {
-  if (n < 1) return cudaErrorInvalidValue;
+// out[q] = sum of parts[q * n .. q * n + n) for q < nq (nq <= 4), in a fixed order whatever the
+// device: chunks of at most 256 x 128 partials per block, then the single-warp Neumaier
+// finalize.  tmp holds 256 * nq doubles.
+static cudaError_t sum_parts(const double* parts, int n, int nq, double* tmp, double* out, cudaStream_t s) {
+  if (n < 1 || nq < 1 || nq > 4) return cudaErrorInvalidValue;
   const int nb = min(256, (n + RED_THREADS - 1) / RED_THREADS);
   const int chunk = (n + nb - 1) / nb;
-  k_sum_chunks<<<nb, RED_THREADS, 0, s>>>(parts, n, chunk, tmp);
-  k_finalize<<<1, 32, 0, s>>>(tmp, nb, 1, out);
+  k_sum_chunks<<<dim3(nb, nq), RED_THREADS, 0, s>>>(parts, n, chunk, tmp);
+  k_finalize<<<1, 32 * nq, 0, s>>>(tmp, nb, nq, out);
   return cudaGetLastError();
+}
+
+cudaError_t launch_sum_parts(const double* parts, int n, double* tmp, double* out, cudaStream_t s) {
+  return sum_parts(parts, n, 1, tmp, out, s);
 }
 
 template <typename S, int NR>
@@ -172,6 +179,14 @@ static cudaError_t clover_impl(const LatDev& L, double* scratch, double* out2, c
   k_clover_qe<S, NR><<<nb, RED_THREADS, 0, s>>>(L.g, f, scratch);
   k_finalize<<<1, 64, 0, s>>>(scratch, nb, 2, out2);
   k_qe_scale<<<1, 1, 0, s>>>(out2, 1.0 / (double)L.g.Vg);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_qe_from_parts(const double* parts, int n, double* tmp, double* out2, double inv_vol,
+                                 cudaStream_t s) {
+  cudaError_t e = sum_parts(parts, n, 2, tmp, out2, s);
+  if (e != cudaSuccess) return e;
+  k_qe_scale<<<1, 1, 0, s>>>(out2, inv_vol);
   return cudaGetLastError();
 }
 

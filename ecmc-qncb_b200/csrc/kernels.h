@@ -70,15 +70,27 @@ cudaError_t launch_plaquette_partials(const LatDev& L, int nblocks, double* scra
 int reduce_threads();
 // out[0] = sum of parts[0 .. n) in a fixed order (two launches); tmp holds 256 doubles.
 cudaError_t launch_sum_parts(const double* parts, int n, double* tmp, double* out, cudaStream_t s);
+// (Q, E) from per-block clover partials: parts[0 .. n) unscaled q sums, parts[n .. 2n) unscaled
+// e sums; out2[0] = Q = sum q / (4 pi^2), out2[1] = E = sum e / 2 * inv_vol.  tmp holds 512
+// doubles.
+cudaError_t launch_qe_from_parts(const double* parts, int n, double* tmp, double* out2, double inv_vol,
+                                 cudaStream_t s);
 
 // ---- flow (k_flow.cu) --------------------------------------------------------------
 // RK3 stage k (1, 2, 3) of Luescher's integrator: reads links from src, the force
 // accumulator z, writes links to dst.
 cudaError_t launch_flow_stage(int stage, const LatDev& src, const LatDev& dst, const AlgDev& z, double eps,
                               cudaStream_t s, int block);
-// The same stage with one thread per site (k_flow_site.cu).
+// The same stage with one thread per site (k_flow_site.cu; FP32 storages).
 cudaError_t launch_flow_site(int stage, const LatDev& src, const LatDev& dst, const AlgDev& z, double eps,
                              cudaStream_t s);
+// Stage 1 with one thread per site that also sums the clover (q, e) of every site of src:
+// parts[0 .. n) and parts[n .. 2n) receive the per-block unscaled sums, n = flow_site_blocks(src)
+// (feed them to launch_qe_from_parts).  FP32 whole lattices; the links are those of
+// launch_flow_site, bit for bit, and each site's (q, e) that of launch_clover_qe.
+int flow_site_blocks(const LatDev& L);
+cudaError_t launch_flow_site_qe(const LatDev& src, const LatDev& dst, const AlgDev& z, double eps, double* parts,
+                                cudaStream_t s);
 
 // Sets the calling thread's qcb_last_error() message; returns code.
 int set_error(int code, const char* msg);

@@ -72,3 +72,27 @@ def test_heatbath_plaquette_rejects_slabs_and_bad_arguments(ctx):
     _lib.check(lib.qcb_lattice_create_slab(ctx.h, (C.c_int * 4)(4, 4, 4, 8), 0, 4, 0, 18, C.byref(s)))
     assert lib.qcb_heatbath_plaquette(s, 6.0, 1, 1, 1, 0, C.byref(out)) == 7
     lib.qcb_lattice_destroy(s)
+
+
+@pytest.mark.parametrize("dims", [(8, 8, 8, 8), (4, 6, 4, 8), (2, 2, 4, 6)])
+@pytest.mark.parametrize("nr", [12, 18])
+def test_flow_measure_fused_qe_matches_clover_kernel_fp32(ctx, dims, nr):
+    """FP32 topo_charge_flowed sums each record's clover inside stage 1 of the next RK3 step
+    (observables_mpi.cpp:153-178 measures before each group of N_rk_steps): every site's
+    (q, e) is the clover kernel's, so the records agree with a replay through qcb_topo_qe and
+    qcb_flow_steps to the rounding of the FP64 sums (1e-10)."""
+    f = qcb.GaugeField(ctx, dims, "fp32", nr)
+    f.hot_start(17)
+    _lib.check(_lib.lib().qcb_heatbath(f.h, 6.0, 5, 1, 17, 0))
+    n_gf, n_rk = 6, 2
+    got = qcb.observables.topo_charge_flowed(f, qcb.GradientFlow(0.02), n_gf, n_rk).reshape(-1, 3)
+    g = qcb.GaugeField(ctx, dims, "fp32", nr)
+    g.copy_from(f)
+    for s in range(n_gf):
+        q, e = qcb.observables.topo_q_e_clover_global(g)
+        assert got[s, 0] == pytest.approx(s * n_rk * 0.02, abs=1e-12)
+        assert abs(got[s, 1] - q) <= 1e-10 * max(1.0, abs(q)), (s, got[s, 1], q)
+        assert abs(got[s, 2] - e) <= 1e-10 * e, (s, got[s, 2], e)
+        _lib.check(_lib.lib().qcb_flow_steps(g.h, 0.02, n_rk))
+    f.close()
+    g.close()
