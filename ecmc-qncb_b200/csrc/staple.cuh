@@ -138,13 +138,26 @@ __device__ __forceinline__ m3<R> staple_sum_rt(const Geom& g, const F& f, const 
   const NbOff o = nb_offsets(g, x);
   const int32_t upmu = sel4(o.up, mu);
   const uint32_t xmu = (uint32_t)((int32_t)x.s + upmu);
+  if constexpr (sizeof(R) == 4) {
+    // FP32: the planes in a loop that is not unrolled (one plane body, as staple_sum_loop)
+#pragma unroll 1
+    for (int k = 0; k < 3; ++k) {
+      const int nu = k + (k >= mu);
+      const int32_t upnu = sel4(o.up, nu), dnnu = sel4(o.dn, nu);
+      const uint32_t xnu = (uint32_t)((int32_t)x.s + upnu);
+      const uint32_t xmunu = (uint32_t)((int32_t)x.s + upmu + dnnu);
+      const uint32_t xmnu = (uint32_t)((int32_t)x.s + dnnu);
+      staple_terms<F, R>(A, f, nu, mu, par, opp, i, cb_index(xmu), cb_index(xnu), cb_index(xmunu), cb_index(xmnu));
+    }
+  } else {
 #pragma unroll
-  for (int nu = 0; nu < 4; ++nu) {
-    if (nu == mu) continue;
-    const uint32_t xnu = (uint32_t)((int32_t)x.s + o.up[nu]);
-    const uint32_t xmunu = (uint32_t)((int32_t)x.s + upmu + o.dn[nu]);
-    const uint32_t xmnu = (uint32_t)((int32_t)x.s + o.dn[nu]);
-    staple_terms<F, R>(A, f, nu, mu, par, opp, i, cb_index(xmu), cb_index(xnu), cb_index(xmunu), cb_index(xmnu));
+    for (int nu = 0; nu < 4; ++nu) {
+      if (nu == mu) continue;
+      const uint32_t xnu = (uint32_t)((int32_t)x.s + o.up[nu]);
+      const uint32_t xmunu = (uint32_t)((int32_t)x.s + upmu + o.dn[nu]);
+      const uint32_t xmnu = (uint32_t)((int32_t)x.s + o.dn[nu]);
+      staple_terms<F, R>(A, f, nu, mu, par, opp, i, cb_index(xmu), cb_index(xnu), cb_index(xmunu), cb_index(xmnu));
+    }
   }
   return A;
 }
