@@ -15,13 +15,13 @@ struct qcb_ecmc {
   qcb_lattice* lat = nullptr;
   qcb_ecmc_params p{};
   uint64_t seed = 0;
-  uint64_t calls = 0;  // sample calls made (the key of the next call's set)
+  uint64_t calls = 0;  // sample calls made (keys the chains' sets in the next call)
   int nb[4] = {0, 0, 0, 0};
   uint32_t n_chains = 0;
   int lanes = 0;               // lanes per chain asked for (0: chosen by the library)
   double2* d_links = nullptr;  // FP64 array-of-structures copy of the lattice
-  double2* d_set = nullptr;
   qcb_ecmc_chain* d_chains = nullptr;
+  double2* d_sx = nullptr;     // per chain: the set element of the current lift (9 double2)
   uint32_t* d_status = nullptr;
   unsigned long long* d_count = nullptr;  // events, lifts, revs
   unsigned long long* h_count = nullptr;  // pinned: 3 counters + status word
@@ -41,8 +41,8 @@ int ecuda(cudaError_t e, const char* what) {
 
 void ecmc_free(qcb_ecmc* e) {
   cudaFree(e->d_links);
-  cudaFree(e->d_set);
   cudaFree(e->d_chains);
+  cudaFree(e->d_sx);
   cudaFree(e->d_status);
   cudaFree(e->d_count);
   cudaFreeHost(e->h_count);
@@ -87,8 +87,8 @@ int qcb_ecmc_create(qcb_lattice* L, const qcb_ecmc_params* p, uint64_t seed, qcb
     return efail(QCB_ERR_CUDA, "cudaSetDevice failed");
   }
   if (cudaMalloc(&e->d_links, link_aos_bytes(L)) != cudaSuccess ||
-      cudaMalloc(&e->d_set, (size_t)ECMC_SET_SIZE * 9 * sizeof(double2)) != cudaSuccess ||
       cudaMalloc(&e->d_chains, (size_t)e->n_chains * sizeof(qcb_ecmc_chain)) != cudaSuccess ||
+      cudaMalloc(&e->d_sx, (size_t)e->n_chains * 9 * sizeof(double2)) != cudaSuccess ||
       cudaMalloc(&e->d_status, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&e->d_count, 3 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMallocHost(&e->h_count, 4 * sizeof(unsigned long long)) != cudaSuccess) {
@@ -151,7 +151,8 @@ int qcb_ecmc_sample_n(qcb_ecmc* e, const int* shifts, int n) {
   qcb_ctx* c = e->ctx;
   EcmcLaunch a;
   a.links = e->d_links;
-  a.set = e->d_set;
+  a.epsilon_set = e->p.epsilon_set;
+  a.sx = e->d_sx;
   a.chains = e->d_chains;
   a.n_chains = e->n_chains;
   for (int d = 0; d < 4; ++d) {
@@ -180,12 +181,7 @@ int qcb_ecmc_sample_n(qcb_ecmc* e, const int* shifts, int n) {
   const int layout = ecmc_layout(e->n_chains, e->lanes);
   for (int k = 0; k < n && err == cudaSuccess; ++k) {
     for (int d = 0; d < 4; ++d) a.cum[d] = ((shifts[4 * k + d] % a.L[d]) + a.L[d]) % a.L[d];
-    err = launch_ecmc_set(e->d_set, e->p.epsilon_set, e->seed, e->calls, c->stream);
-    if (err != cudaSuccess) {
-      what = "ECMC set";
-      break;
-    }
-    c->launches++;
+    a.call = (uint32_t)e->calls;
     err = launch_ecmc_sample(a, layout, c->stream);
     if (err != cudaSuccess) {
       what = "ECMC sample";
@@ -248,9 +244,10 @@ int qcb_ecmc_set_chains(qcb_ecmc* e, const qcb_ecmc_chain* chains, uint64_t call
   for (uint32_t i = 0; i < e->n_chains; ++i) {
     const qcb_ecmc_chain& r = chains[i];
     if (!r.initialized) continue;
-    bool ok = r.mu >= 0 && r.mu < 4 && (r.epsilon == -1 || r.epsilon == 1);
+    bool ok = r.mu >= 0 && r.mu < 4 && (r.epsilon == -1 || r.epsilon == 1) && r.set_counter >= 0 &&
+              r.set_counter <= 10000;
     for (int d = 0; d < 4; ++d) ok = ok && r.site[d] >= -(1 << 20) && r.site[d] <= (1 << 20);
-    if (!ok) return efail(QCB_ERR_INVALID, "chain " + std::to_string(i) + " has a direction, sense or site out of range");
+    if (!ok) return efail(QCB_ERR_INVALID, "chain " + std::to_string(i) + " has a direction, sense, site or set counter out of range");
   }
   qcb_ctx* c = e->ctx;
   std::lock_guard<std::mutex> lk(c->mu);

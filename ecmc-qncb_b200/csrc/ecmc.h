@@ -14,7 +14,6 @@ constexpr int ECMC_SET_SIZE = 10001;
 // One sample call of every chain.
 struct EcmcLaunch {
   double2* links;        // FP64 array-of-structures copy: link (s, mu) = 9 double2 at (4 s + mu) * 9
-  const double2* set;    // ECMC_SET_SIZE matrices of 9 double2
   qcb_ecmc_chain* chains;
   uint32_t n_chains;
   int L[4];              // lattice extents
@@ -24,11 +23,11 @@ struct EcmcLaunch {
   double beta, theta_sample, theta_refresh_site, theta_refresh_R;
   int poisson;
   uint32_t k0, k1;       // Philox key (seed)
+  uint32_t call;         // sample calls made so far (keys the chains' sets)
+  double epsilon_set;    // size of the near-identity set's rotations
+  double2* sx;           // per chain: 9 double2 holding the set element of the current lift
   uint32_t* status;      // OR of the chains' status bits
 };
-
-// The call's set, drawn from Philox counters (j, call_lo, call_hi, set domain).
-cudaError_t launch_ecmc_set(double2* set, double epsilon, uint64_t seed, uint64_t call, cudaStream_t s);
 // Launch shapes of the sample kernel: lanes per chain (1, 3 or 6, each lane computing an
 // equal share of the six staples; lanes 0-2 of a group also share the lift's three products)
 // and the register budget (C: capped for more resident chains).  All give the same results,

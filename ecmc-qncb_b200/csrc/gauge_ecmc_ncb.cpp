@@ -21,9 +21,10 @@
 // reference's frame before a configuration is written.  Differences, by design: chain r
 // draws from Philox4x32-10 keyed by `seed` (its seed file stores the key, its draw count and
 // the number of sample calls; seed file 0 also holds the translations' std::mt19937_64
-// state), the near-identity set is drawn once per shift for all chains,
-// and the state file separates set_counter from event_counter by a space (the reference
-// writes them with no separator, io.cpp:174-175; set_counter is always 0 here).
+// state), each chain's near-identity set is drawn from counters keyed by the chain, the call
+// and the set's renewal count (renewed, as the reference renews its rank's set, at every call
+// and every 10000 lifts), and the state file separates set_counter from event_counter by a
+// space (the reference writes them with no separator, io.cpp:174-175).
 // Optional extra keys: precision = fp64 | fp32, storage = 18 | 12, device = N.
 #include <stdio.h>
 #include <string.h>
@@ -239,7 +240,7 @@ struct Run {
       }
       f << std::setprecision(17);
       f << site << " " << c.mu << " " << c.epsilon << " " << c.travelled_site << " " << c.travelled_R << " "
-        << c.theta_refresh_site << " " << c.theta_refresh_R << " " << 0 << " " << c.events << " " << c.lifts << " "
+        << c.theta_refresh_site << " " << c.theta_refresh_R << " " << c.set_counter << " " << c.events << " " << c.lifts << " "
         << c.revs << " " << " " << (c.initialized != 0) << "\n";
       for (int i = 0; i < 3; ++i) {
         for (int j = 0; j < 3; ++j) f << c.R[2 * (3 * i + j)] << " " << c.R[2 * (3 * i + j) + 1] << " ";
@@ -287,6 +288,7 @@ struct Run {
       c.site[2] = (int)((site / E / E) % E) - 1;
       c.site[3] = (int)(site / E / E / E) - 1;
       c.initialized = init ? 1 : 0;
+      c.set_counter = (int32_t)(set_counter % 10000);
     }
     CHECK(qcb_ecmc_set_chains(ecmc, ch.data(), calls), "ECMC chains");
     std::cout << "Successfully loaded ECMC chain state from: " << state_path(0).parent_path() << std::endl;

@@ -11,9 +11,12 @@
 // costs 5 DRAM sectors where the structure-of-arrays layout costs 9.
 //
 // Random numbers: chain c's k-th uniform is Philox4x32-10 with counter (k_lo, k_hi, c,
-// ECMC_CHAIN) and key seed; the call's set of near-identity elements uses counters
-// (j, call_lo, call_hi, ECMC_SET).  The arithmetic is the reference's up to the order of
-// the floating-point operations (products streamed by rows, dS as a trace against
+// ECMC_CHAIN) and key seed.  Each chain has its own set of near-identity elements, as each
+// rank of the reference has, renewed at the start of every call and whenever its set_counter
+// (lifts since the last renewal) is a multiple of 10000 at the top of the event loop
+// (ecmc_mpi_cb.cpp:560-566); the set is never stored: element pair p of generation gen comes
+// from counters (3p + j, c, call, ECMC_SETC ^ gen), j < 3, when a lift picks it.  The
+// arithmetic is the reference's up to the order of the floating-point operations (products streamed by rows, dS as a trace against
 // R diag(1, -1, 0) R^dagger), so the CPU oracle, drawing from the same counters, takes the
 // same events with links equal to rounding.
 #include <cuda_runtime.h>
@@ -28,7 +31,7 @@
 namespace qcb {
 namespace {
 
-constexpr uint32_t ECMC_CHAIN = 0xECEC0001u, ECMC_SET = 0xECEC0002u;
+constexpr uint32_t ECMC_CHAIN = 0xECEC0001u, ECMC_SETC = 0xECE50000u;
 constexpr uint64_t ECMC_MAX_EVENTS = 1ull << 26;
 constexpr double PI = 3.141592653589793;  // the double nearest pi
 // Sample kernel blocks: two warps.  Register caps: none (255 per thread), or ECMC_CAPPED
@@ -338,43 +341,56 @@ __device__ M embed(const double x[4], int i, int j) {
   return X;
 }
 
-// ecmc_set / random_SU3_epsilon (src/su3/utils.cpp:66-127): thread p writes set[2p+1] =
-// the product of (sqrt(1 - eps^2), eps r/|r|) embedded in (0,1), (0,2), (1,2), r uniform in
-// (-1/2, 1/2)^3, and set[2p+2] = its adjoint; thread 0 also writes set[0] = 1.
-__global__ void k_ecmc_set(double2* set, double eps, uint32_t k0, uint32_t k1, uint32_t call_lo, uint32_t call_hi) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= (ECMC_SET_SIZE - 1) / 2) return;
+// q (9 double2) = element iset of a chain's set (ecmc_set / random_SU3_epsilon,
+// src/su3/utils.cpp:66-127: set[0] = 1, set[2p+1] = the product of (sqrt(1 - eps^2), eps r/|r|)
+// embedded in (0,1), (0,2), (1,2) with r uniform in (-1/2, 1/2)^3, set[2p+2] = its adjoint),
+// generation gen of chain c in call `call`; r from three Philox calls (3p + j, c, call,
+// ECMC_SETC ^ gen).  Each embedding multiplies from the right and changes two columns only;
+// skipping the exact zeros and ones of the embedded matrix leaves every rounding as in the
+// full 3x3 product.
+__device__ __noinline__ void set_elem(double2* q, double eps, uint32_t k0, uint32_t k1, uint32_t c, uint32_t call,
+                                      uint32_t gen, int iset) {
   M Mx;
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
     for (int b = 0; b < 3; ++b) Mx.e[a][b] = mk(a == b ? 1.0 : 0.0, 0.0);
-  if (p == 0)
-    for (int c = 0; c < 9; ++c) set[c] = make_double2(c % 4 == 0 ? 1.0 : 0.0, 0.0);
-  const int sub[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+  if (iset != 0) {
+    const uint32_t p = (uint32_t)(iset - 1) >> 1;
+    double r[12];
 #pragma unroll
-  for (int s = 0; s < 3; ++s) {
-    double r[3];
+    for (uint32_t j = 0; j < 3; ++j) {
+      u32x4 cc;
+      cc.v[0] = 3 * p + j;
+      cc.v[1] = c;
+      cc.v[2] = call;
+      cc.v[3] = ECMC_SETC ^ (gen & 0xFFFFu);
+      const u32x4 w = philox4x32_10(cc, k0, k1);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      u32x4 c;
-      c.v[0] = (uint32_t)(p * 9 + 3 * s + d);
-      c.v[1] = call_lo;
-      c.v[2] = call_hi;
-      c.v[3] = ECMC_SET;
-      const u32x4 w = philox4x32_10(c, k0, k1);
-      r[d] = u53(w.v[0], w.v[1]) - 0.5;
+      for (int t = 0; t < 4; ++t) r[4 * j + t] = ((double)w.v[t] + 0.5) * 2.3283064365386963e-10 - 0.5;
     }
-    const double norm = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-    const double x[4] = {sqrt(1 - eps * eps), eps * r[0] / norm, eps * r[1] / norm, eps * r[2] / norm};
-    Mx = mul_nn(Mx, embed(x, sub[s][0], sub[s][1]));
+    const int sub[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      const double norm = sqrt(r[3 * s] * r[3 * s] + r[3 * s + 1] * r[3 * s + 1] + r[3 * s + 2] * r[3 * s + 2]);
+      const double x0 = sqrt(1 - eps * eps), x1 = eps * r[3 * s] / norm, x2 = eps * r[3 * s + 1] / norm,
+                   x3 = eps * r[3 * s + 2] / norm;
+      const int i = sub[s][0], j = sub[s][1];
+      const Z Eii = mk(x0, x3), Ejj = mk(x0, -x3), Eij = mk(x2, x1), Eji = mk(-x2, x1);
+#pragma unroll
+      for (int row = 0; row < 3; ++row) {
+        const Z a = Mx.e[row][i], b = Mx.e[row][j];
+        Mx.e[row][i] = cfma(b, Eji, cmul(a, Eii));
+        Mx.e[row][j] = cfma(b, Ejj, cmul(a, Eij));
+      }
+    }
   }
-  double2* q = set + (size_t)(2 * p + 1) * 9;
+  const bool adj = iset != 0 && (iset & 1) == 0;
 #pragma unroll
-  for (int c = 0; c < 9; ++c) q[c] = make_double2(Mx.e[c / 3][c % 3].re, Mx.e[c / 3][c % 3].im);
-  q += 9;
-#pragma unroll
-  for (int c = 0; c < 9; ++c) q[c] = make_double2(Mx.e[c % 3][c / 3].re, -Mx.e[c % 3][c / 3].im);
+  for (int k = 0; k < 9; ++k) {
+    const Z v = adj ? mk(Mx.e[k % 3][k / 3].re, -Mx.e[k % 3][k / 3].im) : Mx.e[k / 3][k % 3];
+    q[k] = make_double2(v.re, v.im);
+  }
 }
 
 // sample_persistant (ecmc_mpi_cb.cpp:496-637) for chain c: events until it has travelled
@@ -410,8 +426,9 @@ __global__ void __launch_bounds__(ECMC_WARPS * 32, MINB) k_ecmc_sample(EcmcLaunc
   g.k1 = a.k1;
   g.n = rec.draws;
   const int l = a.l;
-  const double2* set = a.set;
   double2* links = a.links;
+  int set_counter = rec.initialized ? rec.set_counter : 0;
+  uint32_t set_gen = 0;  // renewed at the start of every call
   int lc[4], mu, eps;
   double th_site, th_R, tr_site, tr_R;
   uint64_t events, lifts, revs = rec.revs;
@@ -450,6 +467,10 @@ __global__ void __launch_bounds__(ECMC_WARPS * 32, MINB) k_ecmc_sample(EcmcLaunc
     if (ev >= ECMC_MAX_EVENTS) {
       status |= 2;
       break;
+    }
+    if (set_counter % 10000 == 0) {  // the chain's set is renewed
+      ++set_gen;
+      set_counter = 0;
     }
     const uint32_t x = blk.site(lc);
     // rows 0 and 1 of T = R^dagger U: all the reject angles need
@@ -628,7 +649,10 @@ __global__ void __launch_bounds__(ECMC_WARPS * 32, MINB) k_ecmc_sample(EcmcLaunc
       // plaquette: the proposal R_new = S R is known in advance and its dS rides along
       const double r = g.uni();
       const int iset = (int)(g.uni() * (double)ECMC_SET_SIZE);
-      const double2* sq = set + (size_t)iset * 9;
+      // the picked element, formed once into the chain's slot (every lane of the chain writes
+      // the same values and reads back its own writes)
+      double2* sq = a.sx + (size_t)c * 9;
+      set_elem(sq, a.epsilon_set, a.k0, a.k1, c, a.call, set_gen, iset);
       Herm Qn;
       {
         Z c0[3], c1[3];
@@ -702,6 +726,7 @@ __global__ void __launch_bounds__(ECMC_WARPS * 32, MINB) k_ecmc_sample(EcmcLaunc
       const bool same = t4[0] == lc[0] && t4[1] == lc[1] && t4[2] == lc[2] && t4[3] == lc[3];
       revs += same ? 1 : 0;
       ++lifts;
+      ++set_counter;
 #pragma unroll
       for (int d = 0; d < 4; ++d) lc[d] = t4[d];
       mu = nmu;
@@ -727,6 +752,7 @@ __global__ void __launch_bounds__(ECMC_WARPS * 32, MINB) k_ecmc_sample(EcmcLaunc
   rec.lifts = lifts;
   rec.revs = revs;
   rec.initialized = 1;
+  rec.set_counter = set_counter;
   rec.status = status;
   if (status) atomicOr(a.status, (uint32_t)status);
 }
@@ -755,12 +781,6 @@ __global__ void k_ecmc_counters(qcb_ecmc_chain* chains, uint32_t n, unsigned lon
 
 }  // namespace
 
-cudaError_t launch_ecmc_set(double2* set, double epsilon, uint64_t seed, uint64_t call, cudaStream_t s) {
-  const int pairs = (ECMC_SET_SIZE - 1) / 2;
-  k_ecmc_set<<<(pairs + 127) / 128, 128, 0, s>>>(set, epsilon, (uint32_t)seed, (uint32_t)(seed >> 32),
-                                                 (uint32_t)call, (uint32_t)(call >> 32));
-  return cudaGetLastError();
-}
 
 namespace {
 

@@ -26,7 +26,7 @@ CHAIN_DTYPE = np.dtype([
     ("travelled_site", np.float64), ("travelled_R", np.float64),
     ("draws", np.uint64), ("events", np.uint64), ("lifts", np.uint64), ("revs", np.uint64),
     ("site", np.int32, (4,)), ("mu", np.int32), ("epsilon", np.int32),
-    ("initialized", np.int32), ("status", np.int32), ("pad", np.int32, (4,)),
+    ("initialized", np.int32), ("status", np.int32), ("set_counter", np.int32), ("pad", np.int32, (3,)),
 ])
 assert CHAIN_DTYPE.itemsize == 256
 

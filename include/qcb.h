@@ -377,7 +377,8 @@ typedef struct qcb_ecmc_chain {
   int32_t mu, epsilon;        /* direction of the active link, sense of rotation (+1 / -1) */
   int32_t initialized;        /* 0: drawn at the next call (site, mu, epsilon, R, budgets) */
   int32_t status;             /* latest call: bit 0 non-finite event angle; bit 1 2^26 events */
-  int32_t pad[4];
+  int32_t set_counter;        /* lifts since the chain's near-identity set was renewed */
+  int32_t pad[3];
 } qcb_ecmc_chain;
 int qcb_ecmc_create(qcb_lattice* lat, const qcb_ecmc_params* params, uint64_t seed, qcb_ecmc** out);
 int qcb_ecmc_destroy(qcb_ecmc* e);
@@ -403,7 +404,8 @@ int qcb_ecmc_sample_n(qcb_ecmc* e, const int* shifts, int n);
  * status bits of their latest call. */
 int qcb_ecmc_counters(qcb_ecmc* e, uint64_t out[3], int reset);
 /* Copies the chain records (qcb_ecmc_num_chains of them) and the number of sample calls
- * made so far (the key of the next call's set) to / from host memory; synchronous. */
+ * made so far (which keys the chains' near-identity sets in the next call) to / from host
+ * memory; synchronous. */
 int qcb_ecmc_get_chains(qcb_ecmc* e, qcb_ecmc_chain* chains, uint64_t* calls);
 int qcb_ecmc_set_chains(qcb_ecmc* e, const qcb_ecmc_chain* chains, uint64_t calls);
 

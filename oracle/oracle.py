@@ -118,7 +118,7 @@ def lib():
         L.orc_ref_set_links.argtypes = [C.c_void_p, dp]
         L.orc_ecmc_solve_reject.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, dp]
         L.orc_ecmc_compute_ds.argtypes = [dp, dp, dp]
-        L.orc_ecmc_set.argtypes = [C.c_double, C.c_uint64, C.c_uint64, dp]
+        L.orc_ecmc_set.argtypes = [C.c_double, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, dp]
         L.orc_ecmc_sample.argtypes = [dp, ip, dp, ip, C.c_uint64, C.c_uint64, ip, C.c_void_p]
         L.orc_ecmc_ref_create.argtypes = [C.c_int, C.c_int, C.c_int, dp, ip]
         L.orc_ecmc_ref_create.restype = C.c_void_p
@@ -412,7 +412,7 @@ ECMC_CHAIN_DTYPE = np.dtype([
     ("travelled_site", np.float64), ("travelled_R", np.float64),
     ("draws", np.uint64), ("events", np.uint64), ("lifts", np.uint64), ("revs", np.uint64),
     ("site", np.int32, (4,)), ("mu", np.int32), ("epsilon", np.int32),
-    ("initialized", np.int32), ("status", np.int32), ("pad", np.int32, (4,)),
+    ("initialized", np.int32), ("status", np.int32), ("set_counter", np.int32), ("pad", np.int32, (3,)),
 ])
 assert ECMC_CHAIN_DTYPE.itemsize == 256
 ECMC_SET_SIZE = 10001
@@ -432,9 +432,10 @@ def ecmc_compute_ds(P, R) -> float:
     return out.value
 
 
-def ecmc_set(epsilon, seed, call) -> np.ndarray:
+def ecmc_set(epsilon, seed, call, chain=0, gen=1) -> np.ndarray:
+    """The set of near-identity elements of chain `chain`, generation `gen`, call `call`."""
     out = np.zeros((ECMC_SET_SIZE, 3, 3), np.complex128)
-    lib().orc_ecmc_set(epsilon, C.c_uint64(seed), C.c_uint64(call), _dp(out))
+    lib().orc_ecmc_set(epsilon, C.c_uint64(seed), chain, C.c_uint64(call), gen, _dp(out))
     return out
 
 

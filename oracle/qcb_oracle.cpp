@@ -596,9 +596,12 @@ struct RefChain {
 // its own persistent chain.  The chains are independent: the links a chain reads outside its
 // own active links are frozen in their owners' blocks (GeometryCB.cpp:33-56).  Randomness:
 // chain c's k-th uniform comes from Philox4x32-10 with counter (k_lo, k_hi, c, ECMC_CHAIN) and
-// key = seed; the set of SU(3) elements near the identity (ecmc_set) is drawn once per sample
-// call from counters (j, call_lo, call_hi, ECMC_SET) and shared by all chains.
-const uint32_t ECMC_CHAIN = 0xECEC0001u, ECMC_SET = 0xECEC0002u;
+// key = seed.  Each chain has its own set of SU(3) elements near the identity (ecmc_set), as
+// each rank of the reference has: renewed at the start of every call and whenever the chain's
+// set_counter (lifts since the last renewal) reaches a multiple of 10000 at the top of the event
+// loop (ecmc_mpi_cb.cpp:560-566).  Element pair p of generation gen of chain c in call `call`
+// comes from counters (3p + j, c, call, ECMC_SETC ^ gen), j < 3, so the set is never stored.
+const uint32_t ECMC_CHAIN = 0xECEC0001u, ECMC_SET = 0xECEC0002u, ECMC_SETC = 0xECE50000u;
 const int ECMC_SET_SIZE = 10001;  // sample_persistant's set (ecmc_mpi_cb.cpp:560)
 const uint64_t ECMC_MAX_EVENTS = 1ull << 26;
 
@@ -610,7 +613,8 @@ struct EcmcChain {
   uint64_t draws, events, lifts, revs;
   int32_t site[4];
   int32_t mu, epsilon, initialized, status;
-  int32_t pad[4];
+  int32_t set_counter;  // lifts since the chain's set was last renewed (mod 10000)
+  int32_t pad[3];
 };
 static_assert(sizeof(EcmcChain) == 256, "chain record is 256 bytes");
 
@@ -658,22 +662,6 @@ static M3 su3_near_identity(double eps, const double r[9]) {
     M = mul(M, su2_quaternion_to_su3(x, sub[s][0], sub[s][1]));
   }
   return M;
-}
-
-// ecmc_set (src/su3/utils.cpp:119-127): set[0] = 1, set[2p+1] = random_SU3_epsilon,
-// set[2p+2] = its adjoint.
-static void ecmc_set(double eps, uint64_t seed, uint64_t call, std::vector<M3>& set) {
-  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  set.assign(ECMC_SET_SIZE, ident());
-  for (int p = 0; p < (ECMC_SET_SIZE - 1) / 2; ++p) {
-    double r[9];
-    for (int d = 0; d < 9; ++d) {
-      P4 w = philox({{(uint32_t)(p * 9 + d), (uint32_t)call, (uint32_t)(call >> 32), ECMC_SET}}, k0, k1);
-      r[d] = u53(w.v[0], w.v[1]) - 0.5;
-    }
-    set[2 * p + 1] = su3_near_identity(eps, r);
-    set[2 * p + 2] = adj(set[2 * p + 1]);
-  }
 }
 
 // solve_reject_fast (ecmc_mpi_cb.h:59-94): along U(theta) = R diag(e^{i eps theta},
@@ -753,12 +741,31 @@ static void shifted(const int a[4], int d1, int s1, int d2, int s2, int out[4]) 
   if (d2 >= 0) out[d2] += s2;
 }
 
+// Element iset of a chain's set (ecmc_set, src/su3/utils.cpp:119-127: set[0] = 1,
+// set[2p+1] = random_SU3_epsilon, set[2p+2] = its adjoint) for generation gen of chain c in
+// call `call`, drawn from the counters of element pair p.
+static M3 ecmc_set_elem(double eps, uint32_t k0, uint32_t k1, uint32_t chain, uint32_t call, uint32_t gen, int iset) {
+  if (iset == 0) return ident();
+  const uint32_t pidx = (uint32_t)(iset - 1) >> 1;
+  double r[12];
+  for (uint32_t j = 0; j < 3; ++j) {
+    P4 w = philox({{3 * pidx + j, chain, call, ECMC_SETC ^ (gen & 0xFFFFu)}}, k0, k1);
+    for (int t = 0; t < 4; ++t) r[4 * j + t] = ((double)w.v[t] + 0.5) * 2.3283064365386963e-10 - 0.5;
+  }
+  const M3 M = su3_near_identity(eps, r);
+  return (iset & 1) ? M : adj(M);
+}
+
 // The random draws of one chain, two policies.  LibDraws: the library's counter-based stream
-// (Philox, the call's shared set).  RefDraws (below): the reference's std::mt19937_64 with
-// its std:: distributions and its own set, regenerated as the reference does.
+// (Philox) and the chain's own set, renewed as the reference renews its rank's set.  RefDraws
+// (below): the reference's std::mt19937_64 with its std:: distributions and its own stored
+// set, regenerated as the reference does.
 struct LibDraws {
   EcmcStream g;
-  const std::vector<M3>* set;
+  double eps_set;
+  uint32_t call;
+  int32_t* set_counter;
+  uint32_t gen;
   int l;
   // random_site (ecmc_mpi_cb.cpp:359-367): local coordinates 1 .. l-2 (padded 2 .. L-1)
   void site(int lc[4]) {
@@ -771,16 +778,20 @@ struct LibDraws {
   double gamma() { return -log(g.uni()); }
   double uniform() { return g.uni(); }
   int set_index() { return (int)(g.uni() * (double)ECMC_SET_SIZE); }
-  const M3& set_elem(int i) const { return (*set)[i]; }
-  void call_start() {}
-  void loop_start() {}
-  void on_lift() {}
+  M3 set_elem(int i) const { return ecmc_set_elem(eps_set, g.k0, g.k1, g.chain, call, gen, i); }
+  void call_start() { gen = 0; }
+  void loop_start() {
+    if (*set_counter % 10000 == 0) {
+      ++gen;
+      *set_counter = 0;
+    }
+  }
+  void on_lift() { ++*set_counter; }
 };
 
 // sample_persistant (ecmc_mpi_cb.cpp:496-637) for one chain: events until the chain has
-// travelled theta_sample; the state persists across calls.  The set of near-identity
-// elements is the call's shared set (the reference regenerates its per-rank set at every
-// call and every 10000 lifts).
+// travelled theta_sample; the state persists across calls, the chain's set of near-identity
+// elements is renewed at every call and every 10000 lifts.
 template <class D>
 static void ecmc_chain(const EcmcBlock& blk, const EcmcParams& p, D& g, EcmcChain& st) {
   Lat& f = *blk.f;
@@ -1240,11 +1251,13 @@ int orc_ecmc_compute_ds(const double* p18, const double* r18, double* out) {
   return 0;
 }
 
-// The call's set of ECMC_SET_SIZE matrices (18 doubles each).
-int orc_ecmc_set(double eps, uint64_t seed, uint64_t call, double* out) {
-  std::vector<M3> set;
-  ecmc_set(eps, seed, call, set);
-  for (int i = 0; i < ECMC_SET_SIZE; ++i) memcpy(out + 18 * i, set[i].a, sizeof set[i].a);
+// The whole set (ECMC_SET_SIZE matrices of 18 doubles) of generation gen of chain `chain` in
+// call `call`.
+int orc_ecmc_set(double eps, uint64_t seed, uint32_t chain, uint64_t call, uint32_t gen, double* out) {
+  for (int i = 0; i < ECMC_SET_SIZE; ++i) {
+    const M3 m = ecmc_set_elem(eps, (uint32_t)seed, (uint32_t)(seed >> 32), chain, (uint32_t)call, gen, i);
+    memcpy(out + 18 * i, m.a, sizeof m.a);
+  }
   return 0;
 }
 
@@ -1261,8 +1274,6 @@ int orc_ecmc_sample(double* aos, const int dims[4], const double dp[5], const in
     if (l < 3 || dims[d] % l) return 1;
     nb[d] = dims[d] / l;
   }
-  std::vector<M3> set;
-  ecmc_set(p.epsilon_set, seed, call, set);
   EcmcChain* st = static_cast<EcmcChain*>(chains);
   EcmcBlock blk;
   blk.f = &f;
@@ -1274,7 +1285,9 @@ int orc_ecmc_sample(double* aos, const int dims[4], const double dp[5], const in
       for (int bz = 0; bz < nb[2]; ++bz)
         for (int bt = 0; bt < nb[3]; ++bt, ++id) {
           blk.b[0] = bx, blk.b[1] = by, blk.b[2] = bz, blk.b[3] = bt;
-          LibDraws g{EcmcStream{id, (uint32_t)seed, (uint32_t)(seed >> 32), &st[id].draws}, &set, l};
+          if (!st[id].initialized) st[id].set_counter = 0;
+          LibDraws g{EcmcStream{id, (uint32_t)seed, (uint32_t)(seed >> 32), &st[id].draws}, p.epsilon_set,
+                     (uint32_t)call, &st[id].set_counter, 0u, l};
           ecmc_chain(blk, p, g, st[id]);
         }
   return 0;

@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 # transcendental functions of different libraries resolve differently.
 BASE = dict(beta=6.0, theta_sample=20.0, theta_refresh_site=7.3, theta_refresh_R=3.1, epsilon_set=0.15,
             poisson=0, l_core=4)
-EXACT = ["draws", "events", "lifts", "revs", "site", "mu", "epsilon", "initialized", "status"]
+EXACT = ["draws", "events", "lifts", "revs", "site", "mu", "epsilon", "initialized", "status", "set_counter"]
 
 
 def _compare(rec, ref, tol=1e-9):
@@ -29,6 +29,34 @@ def _compare(rec, ref, tol=1e-9):
         assert np.array_equal(rec[k], ref[k]), k
     for k in ("R", "theta_refresh_site", "theta_refresh_R", "travelled_site", "travelled_R"):
         assert np.abs(rec[k] - ref[k]).max() < tol, k
+
+
+def test_set_renewal_after_10000_lifts_matches_oracle(ctx):
+    """A chain's near-identity set is renewed at the top of the event loop whenever its
+    set_counter is a multiple of 10000 (ecmc_mpi_cb.cpp:560-566), besides the renewal at every
+    call.  Chains restarted with set_counter 9998 renew their set after two lifts inside the
+    call: the GPU takes the oracle's events and ends with the oracle's set_counter."""
+    dims, l = (8, 8, 8, 8), 4
+    p = dict(BASE, l_core=l)
+    u = orc.hot_philox(dims, 31)
+    f = qcb.GaugeField(ctx, dims)
+    f.set_links(u)
+    ch = qcb.EventChains(f, p, 41)
+    ch.sample((1, 2, 0, 3))
+    ref_u, ref_c = orc.ecmc_sample(u, dims, p, 41, 0, (1, 2, 0, 3), orc.ecmc_chains(dims, l))
+    rec, calls = ch.chains()
+    _compare(rec, ref_c)
+    rec["set_counter"] = 9998
+    ref_c["set_counter"] = 9998
+    ch.set_chains(rec, calls)
+    ch.sample((3, 1, 2, 0))
+    ref_u, ref_c = orc.ecmc_sample(ref_u, dims, p, 41, 1, (3, 1, 2, 0), ref_c)
+    rec, _ = ch.chains()
+    _compare(rec, ref_c)
+    assert np.abs(f.get_links() - ref_u).max() < 1e-9
+    assert (rec["set_counter"] < 9998).all()  # every chain lifted at least twice and renewed
+    ch.close()
+    f.close()
 
 
 @pytest.mark.parametrize("dims,l,poisson,beta,eps_set", [((8, 8, 8, 8), 4, 0, 6.0, 0.15),
