@@ -59,13 +59,20 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def fp32_roof(units_per_s, flop_per_unit, peak_tflops):
-    """FP32 operation rate of a kernel from its ncu-counted operations per unit."""
+def fp32_roof(units_per_s, flop_per_unit, peak_tflops, bytes_per_unit=None, hbm_gbs=None):
+    """FP32 operation rate of a kernel from its ncu-counted operations per unit.  With the
+    algorithmic bytes per unit and the HBM peak it also gives the ceiling that the FP32 peak
+    puts on the HBM roofline fraction: units/s at the FP32 peak x bytes per unit / HBM peak."""
     if not flop_per_unit:
         return None
     achieved = units_per_s * flop_per_unit / 1e12
-    return {"achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s", "frac": achieved / peak_tflops,
-            "peak_kind": "nominal", "flop_per_unit": flop_per_unit}
+    out = {"achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s", "frac": achieved / peak_tflops,
+           "peak_kind": "nominal", "flop_per_unit": flop_per_unit}
+    if bytes_per_unit and hbm_gbs:
+        ceiling = peak_tflops * 1e12 / flop_per_unit
+        out["ceiling"] = {"units_per_s_at_fp32_peak": ceiling,
+                          "hbm_frac_at_fp32_peak": ceiling * bytes_per_unit / 1e9 / hbm_gbs}
+    return out
 
 
 def ncu_traffic():
@@ -297,7 +304,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                               "frac": flow_achieved / peak, "peak_kind": peak_kind,
                               "traffic": traffic.get("flow_stage_fp32r12_per_rk3")},
                  "fp32_compute": fp32_roof(V / (rk3_ms / 1e3), traffic.get("flow_fp32r12_fp32_flop_per_site_step"),
-                                           fp32_peak)},
+                                           fp32_peak, FLOW_BYTES[("fp32", 12)], peak)},
         "fp64": {"hb_value": hb64_rate, "flow_value": flow64_rate, "storage": "fp64-18",
                  "hb_speedup_fp32": hb_rate / world / hb64_rate, "flow_speedup_fp32": flow_rate / world / flow64_rate},
         "precision": precision,
@@ -306,7 +313,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist):
                      "traffic": traffic.get("hb_pass_fp32r12_per_launch"),
                      "algorithmic_bytes_per_launch": hb_bytes_launch, "launch_ms": hb_pass_ms,
                      "fp32_compute": fp32_roof(V / 2 / (hb_pass_ms / 1e3),
-                                               traffic.get("hb_pass_fp32r12_fp32_flop_per_link_update"), fp32_peak)},
+                                               traffic.get("hb_pass_fp32r12_fp32_flop_per_link_update"), fp32_peak,
+                                               HB_BYTES[("fp32", 12)], peak)},
         "e2e": {"value": e2e_rate, "unit": "link-updates/s", "ms_per_step": e2e_hb_ms,
                 "h2d_bytes_per_step": V * 72 * 8, "d2h_bytes_per_step": 8,
                 "step": "qcb_set_links from pinned host FP64 links + 500 sweeps + plaquette to host"},
