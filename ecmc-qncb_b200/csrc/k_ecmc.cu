@@ -16,8 +16,8 @@
 // (lifts since the last renewal) is a multiple of 10000 at the top of the event loop
 // (ecmc_mpi_cb.cpp:560-566); the set is never stored: element pair p of generation gen comes
 // from counters (3p + j, c, call, ECMC_SETC ^ gen), j < 3, when a lift picks it.  The
-// arithmetic is the reference's up to the order of the floating-point operations (products streamed by rows, dS as a trace against
-// R diag(1, -1, 0) R^dagger), so the CPU oracle, drawing from the same counters, takes the
+// arithmetic is the reference's up to the order of the floating-point operations (products
+// streamed by rows, dS as a trace against R diag(1, -1, 0) R^dagger), so the CPU oracle, drawing from the same counters, takes the
 // same events with links equal to rounding.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -348,6 +348,17 @@ __device__ M embed(const double x[4], int i, int j) {
 // ECMC_SETC ^ gen).  Each embedding multiplies from the right and changes two columns only;
 // skipping the exact zeros and ones of the embedded matrix leaves every rounding as in the
 // full 3x3 product.
+// Four words of the set's counter stream (one out-of-line copy of the Philox rounds).
+__device__ __noinline__ void set_words(u32x4* w, uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t k0,
+                                       uint32_t k1) {
+  u32x4 cc;
+  cc.v[0] = a;
+  cc.v[1] = b;
+  cc.v[2] = c;
+  cc.v[3] = d;
+  *w = philox4x32_10(cc, k0, k1);
+}
+
 __device__ __noinline__ void set_elem(double2* q, double eps, uint32_t k0, uint32_t k1, uint32_t c, uint32_t call,
                                       uint32_t gen, int iset) {
   M Mx;
@@ -358,17 +369,13 @@ __device__ __noinline__ void set_elem(double2* q, double eps, uint32_t k0, uint3
   if (iset != 0) {
     const uint32_t p = (uint32_t)(iset - 1) >> 1;
     double r[12];
+    u32x4 w[3];
+#pragma unroll 1
+    for (uint32_t j = 0; j < 3; ++j) set_words(&w[j], 3 * p + j, c, call, ECMC_SETC ^ (gen & 0xFFFFu), k0, k1);
 #pragma unroll
-    for (uint32_t j = 0; j < 3; ++j) {
-      u32x4 cc;
-      cc.v[0] = 3 * p + j;
-      cc.v[1] = c;
-      cc.v[2] = call;
-      cc.v[3] = ECMC_SETC ^ (gen & 0xFFFFu);
-      const u32x4 w = philox4x32_10(cc, k0, k1);
+    for (int j = 0; j < 3; ++j)
 #pragma unroll
-      for (int t = 0; t < 4; ++t) r[4 * j + t] = ((double)w.v[t] + 0.5) * 2.3283064365386963e-10 - 0.5;
-    }
+      for (int t = 0; t < 4; ++t) r[4 * j + t] = ((double)w[j].v[t] + 0.5) * 2.3283064365386963e-10 - 0.5;
     const int sub[3][2] = {{0, 1}, {0, 2}, {1, 2}};
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
