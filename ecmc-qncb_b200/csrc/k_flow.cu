@@ -13,6 +13,7 @@
 // previous stage; the force accumulator holds 8 reals per link.
 #include "dispatch.cuh"
 #include "flow_link.cuh"
+#include "sync.cuh"
 
 namespace qcb {
 
@@ -36,6 +37,8 @@ namespace qcb {
 template <typename S, int NR, int STAGE>
 __global__ void __launch_bounds__(128, sizeof(S) == 4 ? QCB_FLOW_MINB32 : QCB_FLOW_MINB64) k_flow_stage(Geom g, Links<S, NR> src, Links<S, NR> dst, AlgField<S> acc,
                                                     S eps) {
+  pdl_launch_dependents();  // launched with programmatic stream serialization
+  pdl_wait();
   const int mu = blockIdx.y;
   const uint32_t i = (blockIdx.x >> 1) * blockDim.x + threadIdx.x;
   const int par = blockIdx.x & 1;
@@ -59,14 +62,18 @@ static cudaError_t flow_impl(int stage, const LatDev& Ls, const LatDev& Ld, cons
   AlgField<S> acc;
   acc.p = reinterpret_cast<typename AlgField<S>::V*>(z.p);
   acc.stride = Ls.g.stride;
-  dim3 grid(grid_for(Ls.g.Vh, block) * 2, 4);
-  if (stage == 1)
-    k_flow_stage<S, NR, 1><<<grid, block, 0, s>>>(Ls.g, src, dst, acc, S(eps));
-  else if (stage == 2)
-    k_flow_stage<S, NR, 2><<<grid, block, 0, s>>>(Ls.g, src, dst, acc, S(eps));
-  else
-    k_flow_stage<S, NR, 3><<<grid, block, 0, s>>>(Ls.g, src, dst, acc, S(eps));
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid_for(Ls.g.Vh, block) * 2, 4);
+  cfg.blockDim = dim3(block);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  void (*kern)(Geom, Links<S, NR>, Links<S, NR>, AlgField<S>, S) =
+      stage == 1 ? k_flow_stage<S, NR, 1> : (stage == 2 ? k_flow_stage<S, NR, 2> : k_flow_stage<S, NR, 3>);
+  return cudaLaunchKernelEx(&cfg, kern, Ls.g, src, dst, acc, S(eps));
 }
 
 // FP32 lattices run the flow with one thread per site (k_flow_site.cu): measured per RK3 step

@@ -9,6 +9,7 @@
 #include "flow_site.cuh"
 #include "obs_site.cuh"
 #include "reduce.cuh"
+#include "sync.cuh"
 
 namespace qcb {
 
@@ -21,6 +22,8 @@ __global__ void __launch_bounds__(FS_THREADS, QCB_FLOW_SITE_MINB) k_flow_site(Ge
                                                                              Links<S, NR> dst, AlgField<S> acc,
                                                                              S eps) {
   extern __shared__ __align__(16) unsigned char fs_smem[];
+  pdl_launch_dependents();  // launched with programmatic stream serialization
+  pdl_wait();
   const int par = blockIdx.x & 1;
   const uint32_t i = (blockIdx.x >> 1) * FS_THREADS + threadIdx.x;
   if (i >= g.Vh) return;
@@ -96,21 +99,24 @@ static cudaError_t flow_site_impl(int stage, const LatDev& Ls, const LatDev& Ld,
   acc.p = reinterpret_cast<typename AlgField<S>::V*>(z.p);
   acc.stride = Ls.g.stride;
   const size_t smem = flow_site_smem<S, NR>();
-  dim3 grid(grid_for(Ls.g.Vh, FS_THREADS) * 2);
+  void (*kern)(Geom, Links<S, NR>, Links<S, NR>, AlgField<S>, S) =
+      stage == 1 ? k_flow_site<S, NR, 1> : (stage == 2 ? k_flow_site<S, NR, 2> : k_flow_site<S, NR, 3>);
   cudaError_t e = cudaSuccess;
-  if (stage == 1) {
-    if (smem > 48 * 1024)
-      e = cudaFuncSetAttribute(k_flow_site<S, NR, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) k_flow_site<S, NR, 1><<<grid, FS_THREADS, smem, s>>>(Ls.g, src, dst, acc, S(eps));
-  } else if (stage == 2) {
-    if (smem > 48 * 1024)
-      e = cudaFuncSetAttribute(k_flow_site<S, NR, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) k_flow_site<S, NR, 2><<<grid, FS_THREADS, smem, s>>>(Ls.g, src, dst, acc, S(eps));
-  } else {
-    if (smem > 48 * 1024)
-      e = cudaFuncSetAttribute(k_flow_site<S, NR, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) k_flow_site<S, NR, 3><<<grid, FS_THREADS, smem, s>>>(Ls.g, src, dst, acc, S(eps));
-  }
+  if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  // programmatic stream serialization: the stage's blocks become resident while the previous
+  // kernel drains (the kernel waits for it before reading)
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid_for(Ls.g.Vh, FS_THREADS) * 2);
+  cfg.blockDim = dim3(FS_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  e = cudaLaunchKernelEx(&cfg, kern, Ls.g, src, dst, acc, S(eps));
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 

@@ -14,6 +14,14 @@ constexpr uint64_t WAIT_NS = 2000000000ull;  // 2 s per wait
 // ends): far above the iterations of a 2 s wait of L2 round trips.
 constexpr uint64_t WAIT_MAX_ITERS = 1ull << 28;
 
+// Programmatic dependent launch (sm_90+): a kernel launched with programmatic stream
+// serialization may be scheduled while the previous kernel of the stream is finishing; it must
+// call pdl_wait() before touching memory the previous kernel writes (the wait ends when that
+// kernel has completed and its writes are visible).  pdl_launch_dependents() lets the next
+// kernel be scheduled once every block of this one has issued it.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
   uint32_t v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
