@@ -56,6 +56,46 @@ def test_slab_hot_start_matches_whole_lattice(ctx):
         assert np.array_equal(s.get_links(), s.local_from_global(whole.get_links()))
 
 
+def test_packed_faces_match_single_face_copies(ctx):
+    """qcb_slab_faces_copy_async packs the faces of every (mu, parity) of one side back to back,
+    in the order of qcb_slab_face_copy, and unpacks them the same way: a packed buffer equals the
+    per-face copies concatenated, and unpacking it into a halo gives that halo the same links."""
+    import torch
+
+    dims = (4, 6, 4, 8)
+    u = orc.hot_philox(dims, 13)
+    for prec, nr in (("fp64", 18), ("fp32", 12)):
+        sl = qs.SlabLattice(ctx, dims, 2, prec, nr)
+        sl.set_links(u)
+        s = sl.slabs[0]
+        ns, nb = s.face_shape()
+        face = ns * nb
+        for mu, par, nf in ((-1, -1, 8), (2, -1, 2), (1, 0, 1)):
+            packed = torch.zeros(nf * face, dtype=torch.uint8, device="cuda")
+            _lib.check(_lib.lib().qcb_slab_faces_copy_async(s.h, qs.LINKS, 1, mu, par, C.c_void_p(packed.data_ptr()), 0))
+            ctx.sync()
+            ref = np.zeros(nf * face, np.uint8)
+            k = 0
+            for m in (range(4) if mu < 0 else [mu]):
+                for p_ in (range(2) if par < 0 else [par]):
+                    s.face_copy(qs.LINKS, 1, m, p_, ref[k * face:].ctypes.data, False)
+                    k += 1
+            assert np.array_equal(packed.cpu().numpy(), ref), (prec, mu, par)
+        # an exchange by hand: the lower slab's last own slice, packed, unpacked into the upper
+        # slab's low halo (first cleared), gives that halo the lower slab's last own slice
+        lo, up = sl.slabs[0], sl.slabs[1]
+        zeros = torch.zeros(8 * face, dtype=torch.uint8, device="cuda")
+        _lib.check(_lib.lib().qcb_slab_faces_copy_async(up.h, qs.LINKS, 0, -1, -1, C.c_void_p(zeros.data_ptr()), 1))
+        ctx.sync()
+        assert not np.array_equal(up.get_links()[0], lo.get_links()[lo.t_local])
+        packed = torch.zeros(8 * face, dtype=torch.uint8, device="cuda")
+        _lib.check(_lib.lib().qcb_slab_faces_copy_async(lo.h, qs.LINKS, 2, -1, -1, C.c_void_p(packed.data_ptr()), 0))
+        _lib.check(_lib.lib().qcb_slab_faces_copy_async(up.h, qs.LINKS, 0, -1, -1, C.c_void_p(packed.data_ptr()), 1))
+        ctx.sync()
+        assert np.array_equal(up.get_links()[0], lo.get_links()[lo.t_local])
+        sl.close()
+
+
 def test_slab_rejects_whole_lattice_calls(ctx):
     s = qs.Slab(ctx, (4, 4, 4, 8), 0, 4)
     lib = _lib.lib()
