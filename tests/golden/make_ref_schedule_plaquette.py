@@ -16,8 +16,10 @@ finite-box deconfinement transition, where a hot start can leave a chain in a me
 with twisted Polyakov-loop sectors (a lower plaquette) for far longer than one chain; an
 ordered start samples one sector, and all sectors have the same plaquette distribution.
 
-Run from the repository root (about 20 minutes on 8 cores):
+Run from the repository root (about 30 minutes on 8 cores):
     python tests/golden/make_ref_schedule_plaquette.py
+or, to regenerate some lattice sizes only and keep the other cases of the existing file:
+    python tests/golden/make_ref_schedule_plaquette.py 4
 """
 import json
 import multiprocessing as mp
@@ -29,7 +31,7 @@ ROOT = HERE.parent.parent
 OUT = HERE / "ref_schedule_plaquette.json"
 
 # (L, n_chains, n_therm, n_sweeps) per lattice size; betas of the statistical oracle.
-SIZES = [(4, 8, 2000, 40000), (8, 16, 1000, 5000)]
+SIZES = [(4, 32, 2000, 40000), (8, 16, 1000, 5000)]
 BETAS = [5.7, 6.0, 6.2]
 # Bins are lengthened by a whole factor until a case has at most this many (longer bins are
 # still at least 10 tau_int), which keeps the file small.
@@ -57,7 +59,12 @@ def main():
     from stats import between_chain_err, chains_summary
 
     oracle.build()
-    jobs = [(L, b, k, th, n) for (L, nc, th, n) in SIZES for b in BETAS for k in range(nc)]
+    only = {int(a) for a in sys.argv[1:]}
+    sizes = [z for z in SIZES if not only or z[0] in only]
+    kept = []
+    if only:
+        kept = [c for c in json.loads(OUT.read_text())["cases"] if c["L"] not in only]
+    jobs = [(L, b, k, th, n) for (L, nc, th, n) in sizes for b in BETAS for k in range(nc)]
     series = {}
     with mp.get_context("spawn").Pool() as pool:
         for key, x in pool.imap_unordered(run_chain, jobs):
@@ -65,7 +72,7 @@ def main():
             print("done", key, flush=True)
     out = {"generator": "tests/golden/make_ref_schedule_plaquette.py", "schedule": "reference (frozen links, "
            "random shift per sweep, lexicographic sweep, mt19937_64, cold start)", "cases": []}
-    for (L, nc, th, n) in SIZES:
+    for (L, nc, th, n) in sizes:
         for b in BETAS:
             chains = [series[(L, b, k)] for k in range(nc)]
             s = chains_summary(chains)
@@ -83,6 +90,7 @@ def main():
             })
             print(f"L={L} beta={b}: {s['mean']:.6f} +- {s['err']:.6f}, tau_int max "
                   f"{max(s['tau_int']):.2f}, bin {s['bin_length']}, {s['n_bins']} bins")
+    out["cases"] = sorted(out["cases"] + kept, key=lambda c: (c["L"], c["beta"]))
     text = json.dumps(out, separators=(",", ":")).replace('{"L"', '\n{"L"')
     OUT.write_text(text + "\n")
 
