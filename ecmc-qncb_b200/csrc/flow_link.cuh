@@ -20,11 +20,11 @@ namespace qcb {
 // per step.  FP64 links are left as the reference leaves them.
 template <typename R>
 __device__ __forceinline__ void flow_reunit(m3<R>& U, int stage) {
-  if constexpr (sizeof(R) == 4) {
+  if constexpr (is_fp32<R>::value) {
     if (stage == 3) {
       m3<double> d = convert<double>(U);
       reunitarize_rows(d);
-      U = convert<float>(d);
+      U = convert<R>(d);
     }
   }
 }
@@ -55,15 +55,15 @@ __device__ __forceinline__ alg8<R> flow_x(const ACC& acc, const alg8<R>& Z, R ep
     alg8<R> N;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      X.a[k] = c1 * Z.a[k] - c0 * Z0.a[k];
-      N.a[k] = R(8.0 / 9.0) * Z.a[k] - R(17.0 / 36.0) * Z0.a[k];
+      X.a[k] = fma(c1, Z.a[k], -(c0 * Z0.a[k]));
+      N.a[k] = fma(R(8.0 / 9.0), Z.a[k], -(R(17.0 / 36.0) * Z0.a[k]));
     }
     acc.template store<R>(MU, par, i, N);
   } else {
     const alg8<R> Z0 = acc.template load<R>(MU, par, i);
     const R c1 = R(0.75) * eps;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) X.a[k] = c1 * Z.a[k] - eps * Z0.a[k];
+    for (int k = 0; k < 8; ++k) X.a[k] = fma(c1, Z.a[k], -(eps * Z0.a[k]));
   }
   return X;
 }
@@ -112,14 +112,14 @@ __device__ __forceinline__ void flow_link_rt(const Geom& g, const F& src, const 
       alg8<R> N;
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        X.a[k] = c1 * Z.a[k] - c0 * Z0.a[k];
-        N.a[k] = R(8.0 / 9.0) * Z.a[k] - R(17.0 / 36.0) * Z0.a[k];
+        X.a[k] = fma(c1, Z.a[k], -(c0 * Z0.a[k]));
+        N.a[k] = fma(R(8.0 / 9.0), Z.a[k], -(R(17.0 / 36.0) * Z0.a[k]));
       }
       acc.template store<R>(mu, par, i, N);
     } else {
       const R c1 = R(0.75) * eps;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) X.a[k] = c1 * Z.a[k] - eps * Z0.a[k];
+      for (int k = 0; k < 8; ++k) X.a[k] = fma(c1, Z.a[k], -(eps * Z0.a[k]));
     }
   }
   const m3<R> E = exp_su3(X);

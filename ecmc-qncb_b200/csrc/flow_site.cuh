@@ -134,14 +134,14 @@ __device__ __forceinline__ void flow_site(const Geom& g, const F& src, const F& 
         alg8<R> N;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          X.a[q] = c1 * Z.a[q] - c0 * Z0.a[q];
-          N.a[q] = R(8.0 / 9.0) * Z.a[q] - R(17.0 / 36.0) * Z0.a[q];
+          X.a[q] = fma(c1, Z.a[q], -(c0 * Z0.a[q]));
+          N.a[q] = fma(R(8.0 / 9.0), Z.a[q], -(R(17.0 / 36.0) * Z0.a[q]));
         }
         acc.template store<R>(mu, par, i, N);
       } else {
         const R c1 = R(0.75) * eps;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) X.a[q] = c1 * Z.a[q] - eps * Z0.a[q];
+        for (int q = 0; q < 8; ++q) X.a[q] = fma(c1, Z.a[q], -(eps * Z0.a[q]));
       }
     }
     const m3<R> E = exp_su3(X);

@@ -27,15 +27,17 @@ struct KpMath<double> {
   static __device__ __forceinline__ void sincos2pi(double u, double* s, double* c) { sincospi(2.0 * u, s, c); }
 };
 template <>
-struct KpMath<float> {
-  static __device__ __forceinline__ float log(float x) { return __logf(x); }
+struct KpMath<f1> {
+  static __device__ __forceinline__ f1 log(f1 x) { return f1(__logf(x.v)); }
   // 2 pi u = 2 pi (u - 1/2) + pi keeps the hardware argument in (-pi, pi).
-  static __device__ __forceinline__ float cos2pi(float u) { return -__cosf(6.28318530717958648f * (u - 0.5f)); }
-  static __device__ __forceinline__ void sincos2pi(float u, float* s, float* c) {
+  static __device__ __forceinline__ f1 cos2pi(f1 u) {
+    return f1(-__cosf(__fmul_rn(6.28318530717958648f, __fsub_rn(u.v, 0.5f))));
+  }
+  static __device__ __forceinline__ void sincos2pi(f1 u, f1* s, f1* c) {
     float sn, cs;
-    __sincosf(6.28318530717958648f * (u - 0.5f), &sn, &cs);
-    *s = -sn;
-    *c = -cs;
+    __sincosf(__fmul_rn(6.28318530717958648f, __fsub_rn(u.v, 0.5f)), &sn, &cs);
+    *s = f1(-sn);
+    *c = f1(-cs);
   }
 };
 
@@ -63,9 +65,9 @@ __device__ __forceinline__ bool kp_draw_inline(R alpha, uint32_t link, uint32_t 
     R r2 = u01<R>(r.v[2]);
     R r3 = u01<R>(r.v[3]);
     R cs = KpMath<R>::cos2pi(r2);
-    R lam2 = mhalf_over_alpha * (KpMath<R>::log(r1) + cs * cs * KpMath<R>::log(r3));
+    R lam2 = mhalf_over_alpha * fma(cs * cs, KpMath<R>::log(r3), KpMath<R>::log(r1));
     if (delta * delta <= R(1) - lam2) {
-      a0 = R(1) - R(2) * lam2;
+      a0 = fma(R(-2), lam2, R(1));
       ok = true;
       break;
     }
@@ -79,9 +81,9 @@ __device__ __forceinline__ bool kp_draw_inline(R alpha, uint32_t link, uint32_t 
   c.v[3] = 0xFFFFFFFFu;
   u32x4 r = philox4x32_10(c, k0, k1);
   R uphi = u01<R>(r.v[0]);
-  R cth = R(2) * u01<R>(r.v[1]) - R(1);
-  R sth = sqrt(fmax(R(0), R(1) - cth * cth));
-  R rs = sqrt(fmax(R(0), R(1) - a0 * a0));
+  R cth = fma(R(2), u01<R>(r.v[1]), R(-1));
+  R sth = sqrt(fmax(R(0), fma(-cth, cth, R(1))));
+  R rs = sqrt(fmax(R(0), fma(-a0, a0, R(1))));
   R sphi, cphi;
   KpMath<R>::sincos2pi(uphi, &sphi, &cphi);
   x[0] = a0;
@@ -115,12 +117,12 @@ __device__ __forceinline__ bool cm_subgroup(m3<R>& U, const m3<R>& A, R beta, ui
   R w1 = (Wab.im + Wba.im) * R(0.5);
   R w2 = (Wab.re - Wba.re) * R(0.5);
   R w3 = (Waa.im - Wbb.im) * R(0.5);
-  R kk = sqrt(w0 * w0 + w1 * w1 + w2 * w2 + w3 * w3);
+  R kk = sqrt(fma(w0, w0, fma(w1, w1, fma(w2, w2, w3 * w3))));
   R ik = R(1) / kk;
   R v0 = w0 * ik, v1 = w1 * ik, v2 = w2 * ik, v3 = w3 * ik;
   R alpha = beta * kk * R(2.0) / R(3.0);
   R x0, x1, x2, x3;
-  if constexpr (sizeof(R) == 8) {
+  if constexpr (std::is_same<R, double>::value) {
     R xq[4];
     if (!kp_draw<R>(alpha, link, sweep, hsg, k0, k1, xq)) return false;
     x0 = xq[0], x1 = xq[1], x2 = xq[2], x3 = xq[3];
@@ -130,10 +132,10 @@ __device__ __forceinline__ bool cm_subgroup(m3<R>& U, const m3<R>& A, R beta, ui
     x0 = xq[0], x1 = xq[1], x2 = xq[2], x3 = xq[3];
   }
   // r = x * adj(v), adj(v) = (v0, -v1, -v2, -v3).
-  R q0 = x0 * v0 + x1 * v1 + x2 * v2 + x3 * v3;
-  R q1 = -x0 * v1 + x1 * v0 - x2 * v3 + x3 * v2;
-  R q2 = -x0 * v2 + x1 * v3 + x2 * v0 - x3 * v1;
-  R q3 = -x0 * v3 - x1 * v2 + x2 * v1 + x3 * v0;
+  R q0 = fma(x0, v0, fma(x1, v1, fma(x2, v2, x3 * v3)));
+  R q1 = fma(-x0, v1, fma(x1, v0, fma(-x2, v3, x3 * v2)));
+  R q2 = fma(-x0, v2, fma(x1, v3, fma(x2, v0, -(x3 * v1))));
+  R q3 = fma(-x0, v3, fma(-x1, v2, fma(x2, v1, x3 * v0)));
   // Embedding: X_aa = q0 + i q3, X_bb = q0 - i q3, X_ab = q2 + i q1, X_ba = -q2 + i q1.
   cx<R> Xaa = mk<R>(q0, q3), Xbb = mk<R>(q0, -q3), Xab = mk<R>(q2, q1), Xba = mk<R>(-q2, q1);
 #pragma unroll

@@ -77,13 +77,13 @@ __device__ __forceinline__ uint32_t hb_item(const BatchRun& run, const BatchLat&
   F f;
   f.p = reinterpret_cast<typename F::V*>(B.links);
   f.stride = B.g.stride;
-  const S beta = S(B.beta);
+  const arith_t<S> beta = arith_t<S>(S(B.beta));
   const int n_hits = B.n_hits > 0 ? B.n_hits : run.n_hits;
   uint32_t fails = 0;
   for (uint32_t k = threadIdx.x; k < B.tile; k += blockDim.x) {
     const uint32_t i = tile * B.tile + k;
     if (i >= B.g.Vh) break;
-    fails += hb_update_link_rt<F, S, NR>(B.g, f, mu, par, i, beta, B.k0, B.k1, sweep, n_hits);
+    fails += hb_update_link_rt<F, arith_t<S>, NR>(B.g, f, mu, par, i, beta, B.k0, B.k1, sweep, n_hits);
   }
   return fails;
 }
@@ -99,7 +99,7 @@ __device__ __forceinline__ uint32_t hb_item(const BatchRun& run, const BatchLat&
 // from register spills and instruction-cache misses.
 template <typename S, int NR>
 __device__ __forceinline__ void flow_item(const BatchRun& run, const BatchLat& B, uint32_t level, uint32_t local,
-                                          S* slot_mem) {
+                                          arith_t<S>* slot_mem) {
   typedef Links<S, NR, LD_CG> F;
   typedef AlgField<S, LD_CG> Z;
   const uint32_t step = level / 3, stage = level - 3 * step;
@@ -112,14 +112,14 @@ __device__ __forceinline__ void flow_item(const BatchRun& run, const BatchLat& B
   Z acc;
   acc.p = reinterpret_cast<typename Z::V*>(B.acc);
   acc.stride = B.g.stride;
-  const S eps = S(B.eps != 0.0 ? B.eps : run.eps);
+  const arith_t<S> eps = arith_t<S>(S(B.eps != 0.0 ? B.eps : run.eps));
   if constexpr (sizeof(S) == 4) {
     const int par = (int)(local & 1);
     const uint32_t tile = local >> 1;
     for (uint32_t k = threadIdx.x; k < B.tile; k += blockDim.x) {
       const uint32_t i = tile * B.tile + k;
       if (i >= B.g.Vh) break;
-      flow_site<F, Z, S, NR>(B.g, src, dst, acc, eps, (int)stage + 1, par, i, slot_mem);
+      flow_site<F, Z, arith_t<S>, NR>(B.g, src, dst, acc, eps, (int)stage + 1, par, i, slot_mem);
     }
   } else {
     const int mp8 = (int)(local & 7), mu = mp8 >> 1, par = mp8 & 1;
@@ -127,7 +127,7 @@ __device__ __forceinline__ void flow_item(const BatchRun& run, const BatchLat& B
     for (uint32_t k = threadIdx.x; k < B.tile; k += blockDim.x) {
       const uint32_t i = tile * B.tile + k;
       if (i >= B.g.Vh) break;
-      flow_link_rt<F, Z, S>(B.g, src, dst, acc, eps, (int)stage + 1, mu, par, i);
+      flow_link_rt<F, Z, arith_t<S>>(B.g, src, dst, acc, eps, (int)stage + 1, mu, par, i);
     }
   }
 }
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(128, sizeof(S) == 4 ? QCB_BATCH_MINB32 : 2) k_
     if (kind == BATCH_HB)
       fails += hb_item<S, NR>(run, B, level, local);
     else
-      flow_item<S, NR>(run, B, level, local, reinterpret_cast<S*>(kb_smem));
+      flow_item<S, NR>(run, B, level, local, reinterpret_cast<arith_t<S>*>(kb_smem));
     block_release(&run.done[l]);
   }
   if (fails) atomicAdd(&run.status[0], fails);
@@ -166,7 +166,7 @@ template <typename S, int NR>
 static cudaError_t batch_launch_impl(int kind, const BatchRun& run, int block, int max_blocks, cudaStream_t s) {
   void* fn = (kind == BATCH_HB) ? (void*)k_batch<S, NR, BATCH_HB>
              : (kind == BATCH_FLOW) ? (void*)k_batch<S, NR, BATCH_FLOW> : (void*)k_batch<S, NR, BATCH_MIXED>;
-  const size_t smem = (sizeof(S) == 4 && kind != BATCH_HB) ? flow_site_smem<S, NR>() : 0;
+  const size_t smem = (sizeof(S) == 4 && kind != BATCH_HB) ? flow_site_smem<arith_t<S>, NR>() : 0;
   int per_sm = 0, dev = 0, sms = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem);
   if (e != cudaSuccess) return e;
@@ -262,10 +262,10 @@ __global__ void __launch_bounds__(RED_SITES, sizeof(S) == 4 ? 4 : 2) k_batch_red
     const uint32_t i = t >> 1;
     const Coord x = cb_coord(B.g, par, i);
     if (WHAT == 0) {
-      v[0] = (double)site_plaquette<Links<S, NR>, S>(B.g, f, x, par, i);
+      v[0] = (double)site_plaquette<Links<S, NR>, arith_t<S>>(B.g, f, x, par, i);
     } else {
-      S q = 0, e = 0;
-      site_qe<Links<S, NR>, S>(B.g, f, x, par, i, &q, &e);
+      arith_t<S> q = 0, e = 0;
+      site_qe<Links<S, NR>, arith_t<S>>(B.g, f, x, par, i, &q, &e);
       v[0] = (double)q;
       v[1] = (double)e;
     }

@@ -44,10 +44,10 @@ __global__ void __launch_bounds__(128, sizeof(S) == 4 ? QCB_FLOW_MINB32 : QCB_FL
   const int par = blockIdx.x & 1;
   if (i >= g.Vh) return;
   switch (mu) {
-    case 0: flow_link<Links<S, NR>, AlgField<S>, S, 0>(g, src, dst, acc, eps, STAGE, par, i); break;
-    case 1: flow_link<Links<S, NR>, AlgField<S>, S, 1>(g, src, dst, acc, eps, STAGE, par, i); break;
-    case 2: flow_link<Links<S, NR>, AlgField<S>, S, 2>(g, src, dst, acc, eps, STAGE, par, i); break;
-    default: flow_link<Links<S, NR>, AlgField<S>, S, 3>(g, src, dst, acc, eps, STAGE, par, i); break;
+    case 0: flow_link<Links<S, NR>, AlgField<S>, arith_t<S>, 0>(g, src, dst, acc, arith_t<S>(eps), STAGE, par, i); break;
+    case 1: flow_link<Links<S, NR>, AlgField<S>, arith_t<S>, 1>(g, src, dst, acc, arith_t<S>(eps), STAGE, par, i); break;
+    case 2: flow_link<Links<S, NR>, AlgField<S>, arith_t<S>, 2>(g, src, dst, acc, arith_t<S>(eps), STAGE, par, i); break;
+    default: flow_link<Links<S, NR>, AlgField<S>, arith_t<S>, 3>(g, src, dst, acc, arith_t<S>(eps), STAGE, par, i); break;
   }
 }
 

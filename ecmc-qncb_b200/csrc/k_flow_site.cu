@@ -27,7 +27,8 @@ __global__ void __launch_bounds__(FS_THREADS, QCB_FLOW_SITE_MINB) k_flow_site(Ge
   const int par = blockIdx.x & 1;
   const uint32_t i = (blockIdx.x >> 1) * FS_THREADS + threadIdx.x;
   if (i >= g.Vh) return;
-  flow_site<Links<S, NR>, AlgField<S>, S, NR>(g, src, dst, acc, eps, STAGE, par, i, reinterpret_cast<S*>(fs_smem));
+  flow_site<Links<S, NR>, AlgField<S>, arith_t<S>, NR>(g, src, dst, acc, arith_t<S>(eps), STAGE, par, i,
+                                                     reinterpret_cast<arith_t<S>*>(fs_smem));
 }
 
 // Stage 1 of a measured RK3 step: the site's four links as k_flow_site, and the clover q and e
@@ -44,10 +45,11 @@ __global__ void __launch_bounds__(FS_THREADS, 4) k_flow_site_qe(Geom g, Links<S,
   const uint32_t i = (blockIdx.x >> 1) * FS_THREADS + threadIdx.x;
   double q = 0.0, e = 0.0;
   if (i < g.Vh) {
-    flow_site<Links<S, NR>, AlgField<S>, S, NR>(g, src, dst, acc, eps, 1, par, i, reinterpret_cast<S*>(fs_smem));
+    flow_site<Links<S, NR>, AlgField<S>, arith_t<S>, NR>(g, src, dst, acc, arith_t<S>(eps), 1, par, i,
+                                                         reinterpret_cast<arith_t<S>*>(fs_smem));
     const Coord x = cb_coord(g, par, i);
-    S qs = 0, es = 0;
-    site_qe<Links<S, NR>, S>(g, src, x, par, i, &qs, &es);
+    arith_t<S> qs = 0, es = 0;
+    site_qe<Links<S, NR>, arith_t<S>>(g, src, x, par, i, &qs, &es);
     q = (double)qs;
     e = (double)es;
   }
@@ -70,7 +72,7 @@ static cudaError_t flow_site_qe_impl(const LatDev& Ls, const LatDev& Ld, const A
   AlgField<S> acc;
   acc.p = reinterpret_cast<typename AlgField<S>::V*>(z.p);
   acc.stride = Ls.g.stride;
-  const size_t smem = flow_site_smem<S, NR>();
+  const size_t smem = flow_site_smem<arith_t<S>, NR>();
   k_flow_site_qe<S, NR><<<dim3(grid_for(Ls.g.Vh, FS_THREADS) * 2), FS_THREADS, smem, s>>>(Ls.g, src, dst, acc, S(eps),
                                                                                         parts);
   return cudaGetLastError();
@@ -98,7 +100,7 @@ static cudaError_t flow_site_impl(int stage, const LatDev& Ls, const LatDev& Ld,
   AlgField<S> acc;
   acc.p = reinterpret_cast<typename AlgField<S>::V*>(z.p);
   acc.stride = Ls.g.stride;
-  const size_t smem = flow_site_smem<S, NR>();
+  const size_t smem = flow_site_smem<arith_t<S>, NR>();
   void (*kern)(Geom, Links<S, NR>, Links<S, NR>, AlgField<S>, S) =
       stage == 1 ? k_flow_site<S, NR, 1> : (stage == 2 ? k_flow_site<S, NR, 2> : k_flow_site<S, NR, 3>);
   cudaError_t e = cudaSuccess;

@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(128, HbMinBlocks<S>::value) k_hb_pass(Geom g, 
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.Vh) return;
   if (FROZEN && is_frozen<MU>(cb_coord(g, par, i), fm)) return;
-  const uint32_t fails = hb_update_link<Links<S, NR>, S, NR, MU>(g, f, par, i, beta, k0, k1, sweep, n_hits);
+  const uint32_t fails = hb_update_link<Links<S, NR>, arith_t<S>, NR, MU>(g, f, par, i, arith_t<S>(beta), k0, k1, sweep, n_hits);
   if (fails) atomicAdd(status, fails);
 }
 
@@ -120,9 +120,9 @@ __global__ void __launch_bounds__(128, HbMinBlocks<S>::value) k_hb_pass_meas(Geo
   uint32_t fails = 0;
   if (i < g.Vh) {
     const Coord x = cb_coord(g, par, i);
-    S retr = 0;
-    fails = hb_update_at<Links<S, NR>, S, NR, 3, true>(g, f, x, par, i, beta, k0, k1, sweep, n_hits, &retr);
-    v = (double)site_plaquette_spatial<Links<S, NR>, S>(g, f, x, par, i);
+    arith_t<S> retr = 0;
+    fails = hb_update_at<Links<S, NR>, arith_t<S>, NR, 3, true>(g, f, x, par, i, arith_t<S>(beta), k0, k1, sweep, n_hits, &retr);
+    v = (double)site_plaquette_spatial<Links<S, NR>, arith_t<S>>(g, f, x, par, i);
     if (par) v += (double)retr;
   }
   if (fails) atomicAdd(status, fails);

@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(RED_THREADS, RedMinBlocks<S>::value) k_plaquet
     const int par = (int)(t & 1);
     const uint32_t i = (uint32_t)(t >> 1);
     const Coord x = cb_coord(g, par, i);
-    if (own_site(g, x.c[3])) acc += (double)site_plaquette<Links<S, NR>, S>(g, f, x, par, i);
+    if (own_site(g, x.c[3])) acc += (double)site_plaquette<Links<S, NR>, arith_t<S>>(g, f, x, par, i);
   }
   double b = block_sum<RED_THREADS>(acc, sh);
   if (threadIdx.x == 0) parts[blockIdx.x] = b;

@@ -82,7 +82,7 @@ __device__ __forceinline__ R re_tr_ah(const ah9<R>& A, const ah9<R>& B) {
     s = fma(A.d[k], B.d[k], s);
     t = fma(A.o[k].re, B.o[k].re, fma(A.o[k].im, B.o[k].im, t));
   }
-  return -s - R(2) * t;
+  return fma(R(-2), t, -s);
 }
 
 // |F|^2 = sum_ij |F_ij|^2 = sum_k d_k^2 + 2 sum_{i<j} |F_ij|^2.
@@ -94,7 +94,7 @@ __device__ __forceinline__ R sqnorm_ah(const ah9<R>& A) {
     s = fma(A.d[k], A.d[k], s);
     t = fma(A.o[k].re, A.o[k].re, fma(A.o[k].im, A.o[k].im, t));
   }
-  return s + R(2) * t;
+  return fma(R(2), t, s);
 }
 
 // Product helpers for the clover leaves.  With 12-real storage a product of two SU(3)

@@ -8,6 +8,7 @@
 // draw is a pure function of (key = seed, counter = (link, sweep, hit/subgroup, draw)),
 // so results do not depend on the launch shape or on how lattices are batched.
 #pragma once
+#include "fp32x.cuh"
 #include <stdint.h>
 
 namespace qcb {
@@ -60,6 +61,10 @@ template <>
 __device__ __forceinline__ float u01<float>(uint32_t w) {
   // ((w >> 8) + 1/2) 2^-24: exact product, one rounding in the add; never 0.
   return fmaf((float)(w >> 8), 5.9604644775390625e-08f, 2.9802322387695312e-08f);
+}
+template <>
+__device__ __forceinline__ f1 u01<f1>(uint32_t w) {
+  return f1(u01<float>(w));
 }
 
 // Counter domains (word 2 of the counter) for the different consumers of the stream.

@@ -120,7 +120,7 @@ __device__ __forceinline__ m3<R> staple_sum_loop(const Geom& g, const F& f, cons
 // The staple of the single-lattice kernels: planes in a loop in FP32, unrolled in FP64.
 template <typename F, typename R, int MU>
 __device__ __forceinline__ m3<R> staple_sum_best(const Geom& g, const F& f, const Coord& x, int par, uint32_t i) {
-  if constexpr (sizeof(R) == 4)
+  if constexpr (is_fp32<R>::value)
     return staple_sum_loop<F, R, MU>(g, f, x, par, i);
   else
     return staple_sum<F, R, MU>(g, f, x, par, i);
@@ -138,7 +138,7 @@ __device__ __forceinline__ m3<R> staple_sum_rt(const Geom& g, const F& f, const 
   const NbOff o = nb_offsets(g, x);
   const int32_t upmu = sel4(o.up, mu);
   const uint32_t xmu = (uint32_t)((int32_t)x.s + upmu);
-  if constexpr (sizeof(R) == 4) {
+  if constexpr (is_fp32<R>::value) {
     // FP32: the planes in a loop that is not unrolled (one plane body, as staple_sum_loop)
 #pragma unroll 1
     for (int k = 0; k < 3; ++k) {

@@ -2,10 +2,13 @@
 //
 // The reference carries this arithmetic in Eigen::Matrix<std::complex<double>,3,3,RowMajor>
 // (src/su3/utils.h:12); here it is plain register arrays so that the compiler keeps every
-// element in registers and fuses multiply-adds.  R is the arithmetic type (float/double).
+// element in registers.  R is the arithmetic type: double, or the explicitly rounded FP32
+// type f1 (fp32x.cuh), for which every multiply-add is the fma() written here.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include "fp32x.cuh"
 
 namespace qcb {
 
@@ -27,12 +30,21 @@ template <typename R>
 __device__ __forceinline__ cx<R> operator-(cx<R> a, cx<R> b) { return mk(a.re - b.re, a.im - b.im); }
 template <typename R>
 __device__ __forceinline__ cx<R> operator*(cx<R> a, cx<R> b) {
-  return mk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+  return mk(fma(a.re, b.re, -(a.im * b.im)), fma(a.re, b.im, a.im * b.re));
 }
 template <typename R>
 __device__ __forceinline__ cx<R> operator*(R s, cx<R> a) { return mk(s * a.re, s * a.im); }
 template <typename R>
 __device__ __forceinline__ cx<R> conj(cx<R> a) { return mk(a.re, -a.im); }
+// acc - a*b
+template <typename R>
+__device__ __forceinline__ cx<R> cfms(cx<R> a, cx<R> b, cx<R> acc) {
+  acc.re = fma(-a.re, b.re, acc.re);
+  acc.re = fma(a.im, b.im, acc.re);
+  acc.im = fma(-a.re, b.im, acc.im);
+  acc.im = fma(-a.im, b.re, acc.im);
+  return acc;
+}
 // acc + a*b
 template <typename R>
 __device__ __forceinline__ cx<R> cfma(cx<R> a, cx<R> b, cx<R> acc) {
@@ -261,12 +273,21 @@ __device__ __forceinline__ R re_tr_na(const m3<R>& a, const m3<R>& b) {
   return s;
 }
 
+// conj(a b - c d), four multiply-adds per component.
+template <typename R>
+__device__ __forceinline__ cx<R> conj_diff(cx<R> a, cx<R> b, cx<R> c, cx<R> d) {
+  // Re(ab - cd) = a.re b.re - a.im b.im - c.re d.re + c.im d.im
+  // -Im(ab - cd) = -a.re b.im - a.im b.re + c.re d.im + c.im d.re
+  return mk(fma(a.re, b.re, fma(-a.im, b.im, fma(-c.re, d.re, c.im * d.im))),
+            fma(-a.re, b.im, fma(-a.im, b.re, fma(c.re, d.im, c.im * d.re))));
+}
+
 // Third row of an SU(3) matrix from its first two: r2 = conj(r0 x r1).
 template <typename R>
 __device__ __forceinline__ void reconstruct_row2(m3<R>& u) {
-  u.e[2][0] = conj(u.e[0][1] * u.e[1][2] - u.e[0][2] * u.e[1][1]);
-  u.e[2][1] = conj(u.e[0][2] * u.e[1][0] - u.e[0][0] * u.e[1][2]);
-  u.e[2][2] = conj(u.e[0][0] * u.e[1][1] - u.e[0][1] * u.e[1][0]);
+  u.e[2][0] = conj_diff(u.e[0][1], u.e[1][2], u.e[0][2], u.e[1][1]);
+  u.e[2][1] = conj_diff(u.e[0][2], u.e[1][0], u.e[0][0], u.e[1][2]);
+  u.e[2][2] = conj_diff(u.e[0][0], u.e[1][1], u.e[0][1], u.e[1][0]);
 }
 
 __device__ __forceinline__ double rsqrt_r(double x) { return 1.0 / sqrt(x); }
@@ -277,7 +298,7 @@ template <typename R>
 __device__ __forceinline__ void reunitarize_rows(m3<R>& u) {
   R n0 = 0;
 #pragma unroll
-  for (int j = 0; j < 3; ++j) n0 += u.e[0][j].re * u.e[0][j].re + u.e[0][j].im * u.e[0][j].im;
+  for (int j = 0; j < 3; ++j) n0 = fma(u.e[0][j].re, u.e[0][j].re, fma(u.e[0][j].im, u.e[0][j].im, n0));
   R inv0 = rsqrt_r(n0);
 #pragma unroll
   for (int j = 0; j < 3; ++j) u.e[0][j] = inv0 * u.e[0][j];
@@ -286,10 +307,10 @@ __device__ __forceinline__ void reunitarize_rows(m3<R>& u) {
 #pragma unroll
   for (int j = 0; j < 3; ++j) d = cfma_cn(u.e[0][j], u.e[1][j], d);
 #pragma unroll
-  for (int j = 0; j < 3; ++j) u.e[1][j] = u.e[1][j] - d * u.e[0][j];
+  for (int j = 0; j < 3; ++j) u.e[1][j] = cfms(d, u.e[0][j], u.e[1][j]);
   R n1 = 0;
 #pragma unroll
-  for (int j = 0; j < 3; ++j) n1 += u.e[1][j].re * u.e[1][j].re + u.e[1][j].im * u.e[1][j].im;
+  for (int j = 0; j < 3; ++j) n1 = fma(u.e[1][j].re, u.e[1][j].re, fma(u.e[1][j].im, u.e[1][j].im, n1));
   R inv1 = rsqrt_r(n1);
 #pragma unroll
   for (int j = 0; j < 3; ++j) u.e[1][j] = inv1 * u.e[1][j];
@@ -361,16 +382,15 @@ __device__ __forceinline__ alg8<R> proj_ta(const m3<R>& m) {
 }
 
 // exp(X) for X in su(3) by Luescher's Cayley-Hamilton / Horner recursion with N = 18
-// Taylor terms (reference: exp_su3_luscher, src/su3/utils.cpp:145-193).  The invariants
-// t = -tr(X^2)/2, d = Re(i det X) and the polynomial coefficients q0, q1, q2 are always
-// evaluated in FP64; the matrix X and the result are in R.  Returns exp(X).
-template <typename R>
-__device__ __forceinline__ m3<R> exp_su3(const alg8<R>& x) {
-  // FP64 copies of the 8 algebra reals.
-  double d0 = x.a[0], d1 = x.a[1], d2 = -(double(x.a[0]) + double(x.a[1]));
-  double ar = x.a[2], ai = x.a[3];  // X01
-  double br = x.a[4], bi = x.a[5];  // X02
-  double cr = x.a[6], ci = x.a[7];  // X12
+// Taylor terms (reference: exp_su3_luscher, src/su3/utils.cpp:145-193):
+// exp(X) = q0 + q1 X + q2 X^2.  The invariants t = -tr(X^2)/2, d = Re(i det X) and the
+// coefficients q0, q1, q2 are always evaluated in FP64 (exp_coef64, from the 8 reals of X);
+// the matrix X and the result are in R.
+__device__ __forceinline__ void exp_coef64(const double (&xa)[8], double (&q)[6]) {
+  double d0 = xa[0], d1 = xa[1], d2 = -(xa[0] + xa[1]);
+  double ar = xa[2], ai = xa[3];  // X01
+  double br = xa[4], bi = xa[5];  // X02
+  double cr = xa[6], ci = xa[7];  // X12
   // t = -1/2 tr X^2 = 1/2 sum_ij |X_ij|^2 for anti-Hermitian X.
   double t = 0.5 * (d0 * d0 + d1 * d1 + d2 * d2) + (ar * ar + ai * ai + br * br + bi * bi + cr * cr + ci * ci);
   // det X with X = [[i d0, a, b], [-a*, i d1, c], [-b*, -c*, i d2]]:
@@ -410,6 +430,31 @@ __device__ __forceinline__ m3<R> exp_su3(const alg8<R>& x) {
     q1r = n1r;
     q1i = n1i;
   }
+  q[0] = q0r;
+  q[1] = q0i;
+  q[2] = q1r;
+  q[3] = q1i;
+  q[4] = q2r;
+  q[5] = q2i;
+}
+
+// q0, q1, q2 of exp(X) in R.
+template <typename R>
+__device__ __forceinline__ void exp_coef(const alg8<R>& x, cx<R>& q0, cx<R>& q1, cx<R>& q2) {
+  double xa[8], q[6];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) xa[k] = (double)x.a[k];
+  exp_coef64(xa, q);
+  q0 = mk<R>(R(q[0]), R(q[1]));
+  q1 = mk<R>(R(q[2]), R(q[3]));
+  q2 = mk<R>(R(q[4]), R(q[5]));
+}
+
+// Returns exp(X).
+template <typename R>
+__device__ __forceinline__ m3<R> exp_su3(const alg8<R>& x) {
+  cx<R> q0, q1, q2;
+  exp_coef(x, q0, q1, q2);
   m3<R> X = alg_to_m3(x);
   // X^2 is Hermitian (X^dag = -X); its entries in closed form from the 8 reals
   // (d2 = -d0 - d1; a = X01, b = X02, c = X12):
@@ -419,13 +464,16 @@ __device__ __forceinline__ m3<R> exp_su3(const alg8<R>& x) {
   {
     const R D0 = x.a[0], D1 = x.a[1], D2 = -(x.a[0] + x.a[1]);
     const R Ar = x.a[2], Ai = x.a[3], Br = x.a[4], Bi = x.a[5], Cr = x.a[6], Ci = x.a[7];
-    const R na = Ar * Ar + Ai * Ai, nb = Br * Br + Bi * Bi, nc = Cr * Cr + Ci * Ci;
-    X2.e[0][0] = mk<R>(-(D0 * D0 + na + nb), R(0));
-    X2.e[1][1] = mk<R>(-(D1 * D1 + na + nc), R(0));
-    X2.e[2][2] = mk<R>(-(D2 * D2 + nb + nc), R(0));
-    const cx<R> s01 = mk<R>(D2 * Ai - (Br * Cr + Bi * Ci), -D2 * Ar - (Bi * Cr - Br * Ci));
-    const cx<R> s02 = mk<R>(D1 * Bi + Ar * Cr - Ai * Ci, -D1 * Br + Ar * Ci + Ai * Cr);
-    const cx<R> s12 = mk<R>(D0 * Ci - (Ar * Br + Ai * Bi), -D0 * Cr - (Ar * Bi - Ai * Br));
+    const R na = fma(Ar, Ar, Ai * Ai), nb = fma(Br, Br, Bi * Bi), nc = fma(Cr, Cr, Ci * Ci);
+    X2.e[0][0] = mk<R>(-fma(D0, D0, na + nb), R(0));
+    X2.e[1][1] = mk<R>(-fma(D1, D1, na + nc), R(0));
+    X2.e[2][2] = mk<R>(-fma(D2, D2, nb + nc), R(0));
+    // s01 = (D2 Ai - Br Cr - Bi Ci, -D2 Ar - Bi Cr + Br Ci)
+    const cx<R> s01 = mk<R>(fma(D2, Ai, fma(-Br, Cr, -(Bi * Ci))), fma(-D2, Ar, fma(-Bi, Cr, Br * Ci)));
+    // s02 = (D1 Bi + Ar Cr - Ai Ci, -D1 Br + Ar Ci + Ai Cr)
+    const cx<R> s02 = mk<R>(fma(D1, Bi, fma(Ar, Cr, -(Ai * Ci))), fma(-D1, Br, fma(Ar, Ci, Ai * Cr)));
+    // s12 = (D0 Ci - Ar Br - Ai Bi, -D0 Cr - Ar Bi + Ai Br)
+    const cx<R> s12 = mk<R>(fma(D0, Ci, fma(-Ar, Br, -(Ai * Bi))), fma(-D0, Cr, fma(-Ar, Bi, Ai * Br)));
     X2.e[0][1] = s01;
     X2.e[0][2] = s02;
     X2.e[1][2] = s12;
@@ -433,7 +481,6 @@ __device__ __forceinline__ m3<R> exp_su3(const alg8<R>& x) {
     X2.e[2][0] = conj(s02);
     X2.e[2][1] = conj(s12);
   }
-  cx<R> q0 = mk<R>(R(q0r), R(q0i)), q1 = mk<R>(R(q1r), R(q1i)), q2 = mk<R>(R(q2r), R(q2i));
   m3<R> E;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
