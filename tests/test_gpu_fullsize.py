@@ -66,3 +66,20 @@ def test_flow_energy_decreases_at_32x4_fp32(ctx):
     assert np.all(np.diff(rec[:, 2]) < 0)
     assert np.array_equal(f.get_links(), before)
     f.close()
+
+
+def test_heatbath_and_flow_deterministic_at_32x4_fp32(ctx):
+    """The same seed gives the same links, bit for bit, whatever the block size of the passes
+    (the Philox draws are keyed by link, sweep, hit and subgroup, not by thread)."""
+    lib = qcb._lib.lib()
+    outs = []
+    for block in (128, 64, 128):
+        ctx.set_block(block)
+        f = qcb.GaugeField(ctx, DIMS, "fp32", 12)
+        f.hot_start(5)
+        qcb._lib.check(lib.qcb_heatbath(f.h, 6.0, 5, 1, 5, 0))
+        qcb._lib.check(lib.qcb_flow_steps(f.h, 0.02, 4))
+        outs.append(f.get_links())
+        f.close()
+    ctx.set_block(0)
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
