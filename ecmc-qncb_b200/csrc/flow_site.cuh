@@ -81,20 +81,31 @@ __device__ __forceinline__ void flow_site(const Geom& g, const F& src, const F& 
       const uint32_t ixmnu = cb_index((uint32_t)((int32_t)x.s + dnnu));
       const uint32_t ixmunu = cb_index((uint32_t)((int32_t)x.s + upmu + dnnu));
       // forward: T_{mu nu} U_nu(x)^dagger, T shared with the plane's other link
-      {
+      // 12-real: the forward term W is in SU(3); only its rows 0 and 1 are multiplied out
+      // (T U_nu(x)^dag from T's rows 0, 1; for nu < mu, W = U_nu(x) T from U_nu(x)'s stored
+      // rows, A += W^dag) and its row 2 is rebuilt
+      if constexpr (NR == 12) {
+        if (nu > mu) {
+          const m3<R> U0 = src.template load_rows01<R>(nu, opp, ixmu);
+          const m3<R> U1 = src.template load<R>(mu, opp, ixnu);
+          const m3<R> T = mul_na_rows01(U0, U1);
+          slots.put(t_slot(mu, nu), T);
+          const m3<R> U2 = src.template load<R>(nu, par, i);
+          m3<R> W = mul_na_rows01(T, U2);
+          reconstruct_row2(W);
+          add_m3(A, W);
+        } else {
+          const m3<R> T = slots.get(t_slot(nu, mu));
+          const m3<R> U2 = src.template load_rows01<R>(nu, par, i);
+          m3<R> W = mul_nn_rows01(U2, T);
+          reconstruct_row2(W);
+          add_m3_adj(A, W);
+        }
+      } else {
         const m3<R> U2 = src.template load<R>(nu, par, i);
         if (nu > mu) {
-          m3<R> T;
-          if constexpr (NR == 12) {
-            const m3<R> U0 = src.template load_rows01<R>(nu, opp, ixmu);
-            const m3<R> U1 = src.template load<R>(mu, opp, ixnu);
-            T = mul_na_rows01(U0, U1);
-            slots.put(t_slot(mu, nu), T);
-            reconstruct_row2(T);
-          } else {
-            T = mul_na(src.template load<R>(nu, opp, ixmu), src.template load<R>(mu, opp, ixnu));
-            slots.put(t_slot(mu, nu), T);
-          }
+          m3<R> T = mul_na(src.template load<R>(nu, opp, ixmu), src.template load<R>(mu, opp, ixnu));
+          slots.put(t_slot(mu, nu), T);
           acc_na(A, T, U2);
         } else {
           const m3<R> T = slots.get(t_slot(nu, mu));  // T_{nu mu} = T_{mu nu}^dagger

@@ -31,11 +31,13 @@ __device__ __forceinline__ int32_t sel4(const int32_t* v, int k) {
 
 // The two staple terms of one plane (mu, nu), added to A.  Site indices: i = x (parity
 // par); ixmu = x+mu, ixnu = x+nu, ixmnu = x-nu (parity opp); ixmunu = x+mu-nu (parity par).
-// With 12-real storage each three-link product is an SU(3) matrix whose third row follows
-// from its first two, so only rows 0 and 1 of the first product are computed (from the
-// stored rows of the leading link, with no reconstruction of that link) and row 2 is
-// rebuilt once: forward T = U_nu(x+mu) U_mu(x+nu)^dag, A += T U_nu(x)^dag; backward
-// P = U_mu(x-nu) U_nu(x+mu-nu), A += P^dag U_nu(x-nu).
+// With 12-real storage each product of links is an SU(3) matrix whose third row follows
+// from its first two, so only rows 0 and 1 of a product are computed and row 2 is rebuilt by
+// the cross product.  Forward: rows 0, 1 of T = U_nu(x+mu) U_mu(x+nu)^dag (from the stored
+// rows of U_nu(x+mu)), then rows 0, 1 of W = T U_nu(x)^dag (from rows 0, 1 of T: T's row 2
+// is never formed), W's row 2 rebuilt, A += W.  Backward: P = U_mu(x-nu) U_nu(x+mu-nu) as
+// rows 0, 1 plus the rebuilt row 2, A += P^dag U_nu(x-nu) (this product needs every row of
+// both factors).
 template <typename F, typename R>
 __device__ __forceinline__ void staple_terms(m3<R>& A, const F& f, int nu, int mu, int par, int opp, uint32_t i,
                                              uint32_t ixmu, uint32_t ixnu, uint32_t ixmunu, uint32_t ixmnu) {
@@ -43,10 +45,11 @@ __device__ __forceinline__ void staple_terms(m3<R>& A, const F& f, int nu, int m
     {
       const m3<R> U0 = f.template load_rows01<R>(nu, opp, ixmu);
       const m3<R> U1 = f.template load<R>(mu, opp, ixnu);
-      m3<R> T = mul_na_rows01(U0, U1);
-      reconstruct_row2(T);
+      const m3<R> T = mul_na_rows01(U0, U1);
       const m3<R> U2 = f.template load<R>(nu, par, i);
-      acc_na(A, T, U2);
+      m3<R> W = mul_na_rows01(T, U2);
+      reconstruct_row2(W);
+      add_m3(A, W);
     }
     {
       const m3<R> V1 = f.template load_rows01<R>(mu, opp, ixmnu);

@@ -252,6 +252,21 @@ __device__ __forceinline__ m3<R> mul_nn_rows01(const m3<R>& a, const m3<R>& b) {
     }
   return c;
 }
+// acc += w; acc += w^dagger
+template <typename R>
+__device__ __forceinline__ void add_m3(m3<R>& acc, const m3<R>& w) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) acc.e[i][j] = acc.e[i][j] + w.e[i][j];
+}
+template <typename R>
+__device__ __forceinline__ void add_m3_adj(m3<R>& acc, const m3<R>& w) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) acc.e[i][j] = acc.e[i][j] + conj(w.e[j][i]);
+}
 // Re tr(a * b)
 template <typename R>
 __device__ __forceinline__ R re_tr_nn(const m3<R>& a, const m3<R>& b) {
