@@ -51,10 +51,37 @@ struct TSlots {
   }
 };
 
-// Shared-memory bytes of the T slots of a block.
+// Row 2 of the site's own links U_nu(x), nu = 0..3 (12-real): rebuilt once, in the first
+// direction's pass over the site (mu = 0 uses all four as full matrices), and read back for the
+// later directions.  [4][6][FS_THREADS] after the T slots.
+template <typename R>
+struct Row2Cache {
+  R* base;
+  __device__ __forceinline__ R* at(int nu, int k) const { return base + (nu * 6 + k) * FS_THREADS + threadIdx.x; }
+  // U_nu(x) as a full matrix from its stored rows: row 2 rebuilt and kept when `first`, read
+  // back otherwise.
+  template <typename F>
+  __device__ __forceinline__ m3<R> load(const F& f, int nu, int par, uint32_t i, bool first) const {
+    m3<R> u = f.template load_rows01<R>(nu, par, i);
+    if (first) {
+      reconstruct_row2(u);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        *at(nu, 2 * c) = u.e[2][c].re;
+        *at(nu, 2 * c + 1) = u.e[2][c].im;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) u.e[2][c] = mk<R>(*at(nu, 2 * c), *at(nu, 2 * c + 1));
+    }
+    return u;
+  }
+};
+
+// Shared-memory bytes of the T slots of a block (and, for 12-real, the row-2 cache).
 template <typename R, int NR>
 constexpr size_t flow_site_smem() {
-  return (size_t)4 * (NR == 12 ? 12 : 18) * FS_THREADS * sizeof(R);
+  return (size_t)4 * (NR == 12 ? 12 : 18) * FS_THREADS * sizeof(R) + (NR == 12 ? (size_t)4 * 6 * FS_THREADS * sizeof(R) : 0);
 }
 
 // Stage `stage` (1, 2, 3) of the four links of site x = (par, i): src -> dst.
@@ -63,6 +90,7 @@ __device__ __forceinline__ void flow_site(const Geom& g, const F& src, const F& 
                                           int par, uint32_t i, R* slot_mem) {
   constexpr int TS = NR == 12 ? 12 : 18;
   const TSlots<R, TS> slots{slot_mem};
+  const Row2Cache<R> own{slot_mem + 4 * TS * FS_THREADS};
   const int opp = par ^ 1;
   const Coord x = cb_coord(g, par, i);
   if (!own_site(g, x.c[3])) return;  // halo slice of a slab
@@ -90,7 +118,7 @@ __device__ __forceinline__ void flow_site(const Geom& g, const F& src, const F& 
           const m3<R> U1 = src.template load<R>(mu, opp, ixnu);
           const m3<R> T = mul_na_rows01(U0, U1);
           slots.put(t_slot(mu, nu), T);
-          const m3<R> U2 = src.template load<R>(nu, par, i);
+          const m3<R> U2 = own.load(src, nu, par, i, mu == 0);
           m3<R> W = mul_na_rows01(T, U2);
           reconstruct_row2(W);
           add_m3(A, W);
@@ -128,7 +156,11 @@ __device__ __forceinline__ void flow_site(const Geom& g, const F& src, const F& 
         acc_nn(A, P, V2);
       }
     }
-    const m3<R> U = src.template load<R>(mu, par, i);
+    m3<R> U;
+    if constexpr (NR == 12)
+      U = own.load(src, mu, par, i, mu == 0);
+    else
+      U = src.template load<R>(mu, par, i);
     alg8<R> Z = proj_ta(mul_nn(U, A));
 #pragma unroll
     for (int q = 0; q < 8; ++q) Z.a[q] = -Z.a[q];

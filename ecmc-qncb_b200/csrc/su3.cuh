@@ -501,9 +501,16 @@ __device__ __forceinline__ m3<R> exp_su3(const alg8<R>& x) {
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      cx<R> v = q1 * X.e[i][j];
-      v = cfma(q2, X2.e[i][j], v);
-      if (i == j) v = v + q0;
+      cx<R> v;
+      if (i == j) {
+        // X_ii = i d_i is imaginary and (X^2)_ii real: the products with their zero parts
+        // (which leave the sums unchanged) are left out
+        v = mk<R>(fma(q2.re, X2.e[i][i].re, -(q1.im * X.e[i][i].im)), fma(q2.im, X2.e[i][i].re, q1.re * X.e[i][i].im));
+        v = v + q0;
+      } else {
+        v = q1 * X.e[i][j];
+        v = cfma(q2, X2.e[i][j], v);
+      }
       E.e[i][j] = v;
     }
   return E;
